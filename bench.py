@@ -1,0 +1,473 @@
+#!/usr/bin/env python
+"""Throughput of the fused D3Q19 step on B200 (MLUPS), one JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl wt|reference]
+
+Workload (default): the 256x128x128 channel with a 15-degree-yawed
+superellipsoid hull (80x30x24 cells), u0 = 0.06, Re = 2000 on the length
+(tau = 0.5072), TRT Lambda = 3/16, Smagorinsky Cs = 0.1, free-slip side
+planes, seeded +-1e-4 velocity noise. A "step" is one lattice time step
+over all 4,194,304 cells; MLUPS counts every cell (the reference's
+convention, js/main.js:621).
+
+* value      kernel throughput: K steps of one wt_step call, inputs resident
+             in HBM, CUDA events on the library's stream.
+* e2e        the same metric through the public per-step call a host makes
+             (LBM.step(): parameters pushed, one step, the force read back
+             to host memory, synchronous).
+* fp16dev    the half-deviation storage form on the same workload.
+* accuracy   pair-averaged Cd / Cl of FP32, FP16-dev and FP64 storage after
+             the workload's 10000 steps (average over the last 2000).
+* roofline   152 (FP32) algorithmic bytes per cell update over the measured
+             HBM copy bandwidth.
+* cpu_baseline  the CPU oracle (the reference arithmetic in C, OpenMP z-slabs
+             as js/pool.js decomposes them) timed on this host's cores.
+
+--impl reference times that CPU implementation alone on the same workload.
+Multi-GPU (torchrun): every rank runs an independent replica (the reference
+has no exchange step to shard); value = all cells of all ranks / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = ("MLUPS FP32 vs FP16-store at |ΔCd|<1% vs FP64; "
+          "adjoint grad time / forward time")
+BYTES_PER_CELL = {"f32": 152, "f16dev": 76, "f64": 304}
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    "channel256": dict(
+        name="256x128x128 D3Q19 channel, yawed superellipsoid hull",
+        nx=256, ny=128, nz=128, u0=0.06, tau=0.5072, csm=0.1, lam=3 / 16, les=True,
+        side_bc="freeslip", body=dict(semi=(0.5, 0.1875, 0.15), exponent=2.5, res=160,
+                                      scale=80.0, yaw_deg=15.0), seed=1234, amp=1e-4,
+        accuracy_steps=10000, accuracy_window=2000),
+    "channel512": dict(
+        name="512x192x192 D3Q19 channel, yawed superellipsoid hull x2",
+        nx=512, ny=192, nz=192, u0=0.06, tau=0.5072, csm=0.1, lam=3 / 16, les=True,
+        side_bc="freeslip", body=dict(semi=(0.5, 0.1875, 0.15), exponent=2.5, res=160,
+                                      scale=160.0, yaw_deg=15.0), seed=1234, amp=1e-4,
+        accuracy_steps=8000, accuracy_window=2000),
+}
+
+
+# ---------------------------------------------------------------------------- set-up
+def body_inputs(wl):
+    from windtunnel_b200.bodies import body_box, body_matrix, superellipsoid_grid
+    b = wl["body"]
+    vg = superellipsoid_grid(b["semi"], b["exponent"], b["res"])
+    M = body_matrix(math.radians(b["yaw_deg"]), 0.0)
+    P = [0.36 * wl["nx"], 0.5 * wl["ny"], 0.5 * wl["nz"]]
+    box = body_box(M, vg.ext, b["scale"], P)
+    return vg, M, P, box
+
+
+def setup_gpu(wl, storage, math_mode="fast"):
+    from windtunnel_b200 import LBM
+    sim = LBM(wl["nx"], wl["ny"], wl["nz"], storage=storage, math=math_mode,
+              side_bc=wl["side_bc"])
+    sim.set_params(u0=wl["u0"], tau=wl["tau"], csm=wl["csm"], les=int(wl["les"]),
+                   **{"lambda": wl["lam"]})
+    vg, M, P, box = body_inputs(wl)
+    sim.voxelize_grid(vg.grid, vg.min, vg.inv, M, P, wl["body"]["scale"], box)
+    sim.init_eq_noise(wl["seed"], wl["amp"])
+    return sim
+
+
+def setup_oracle(wl):
+    from oracle.oracle import OracleLBM, lookup_mask
+    o = OracleLBM(wl["nx"], wl["ny"], wl["nz"], "f32", side_bc=wl["side_bc"])
+    o.set_params(u0=wl["u0"], tau=wl["tau"], csm=wl["csm"], les=int(wl["les"]),
+                 **{"lambda": wl["lam"]})
+    vg, M, P, box = body_inputs(wl)
+    mask = lookup_mask(vg.grid, vg.min, vg.inv, M, P, wl["body"]["scale"], wl["nx"], wl["ny"],
+                       wl["nz"], box)
+    o.voxelize_mask(box, mask)
+    o.init_eq_noise(wl["seed"], wl["amp"])
+    return o
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return self
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+        time.sleep(0.3)   # first sample before the region starts
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=5)
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "power_w_max": max(power) if power else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------- helpers
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(kernel_tag: str) -> float | None:
+    """DRAM bytes per launch from the committed ncu summary of this kernel, if any."""
+    p = ROOT / "profiles" / f"{kernel_tag}.md"
+    try:
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+
+    def init(self):
+        import torch
+        torch.cuda.set_device(self.local)
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+def timed_steps(sim, K: int, dist: Dist) -> tuple[float, int]:
+    """K steps in one wt_step call, CUDA events on the library stream; (ms, launches)."""
+    import torch
+    stream = torch.cuda.ExternalStream(sim.stream)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = sim.launch_count
+    dist.barrier()
+    torch.cuda.synchronize()
+    start.record(stream)
+    sim.step_forces(K)
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    dist.barrier()
+    return start.elapsed_time(end), sim.launch_count - l0
+
+
+def e2e_steps(sim, K: int, dist: Dist) -> float:
+    """K public per-step calls: push parameters, step, read the force to host."""
+    import torch
+    stream = torch.cuda.ExternalStream(sim.stream)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p = sim.params()
+    dist.barrier()
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(K):
+        sim.set_params(u0=p.u0, tau=p.tau)   # the host's per-step parameter push
+        sim.step()
+        _ = sim.force                         # force of this step, in host memory
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    dist.barrier()
+    return start.elapsed_time(end)
+
+
+def pair_avg_coeff(forces, u0, area, window):
+    import numpy as np
+    f = np.asarray(forces, np.float64)
+    pa = 0.5 * (f[1:] + f[:-1])
+    q = 0.5 * u0 * u0 * area
+    w = pa[-window:]
+    return float(w[:, 0].mean() / q), float(w[:, 1].mean() / q)
+
+
+def accuracy_study(wl) -> dict:
+    """Cd / Cl of FP32, FP16-dev and FP64 storage after the workload's full step count."""
+    out = {"steps": wl["accuracy_steps"], "window": wl["accuracy_window"],
+           "average": "pair-averaged consecutive steps (js/main.js:113-127)"}
+    coeffs = {}
+    for storage, mm in (("f64", "exact"), ("f32", "fast"), ("f16dev", "fast")):
+        sim = setup_gpu(wl, storage, mm)
+        t0 = time.time()
+        F = sim.step_forces(wl["accuracy_steps"])
+        cd, cl = pair_avg_coeff(F, wl["u0"], sim.frontalArea, wl["accuracy_window"])
+        coeffs[storage] = (cd, cl)
+        out[storage] = {"cd": cd, "cl": cl, "wall_s": round(time.time() - t0, 2)}
+        sim.close()
+    cd64 = coeffs["f64"][0]
+    for s in ("f32", "f16dev"):
+        out[s]["dcd_rel_vs_f64"] = abs(coeffs[s][0] - cd64) / abs(cd64)
+        out[s]["dcl_vs_f64_over_cd"] = abs(coeffs[s][1] - coeffs["f64"][1]) / abs(cd64)
+    out["f16dev"]["dcd_rel_vs_f32"] = abs(coeffs["f16dev"][0] - coeffs["f32"][0]) / abs(
+        coeffs["f32"][0])
+    return out
+
+
+def cpu_baseline(wl, budget_s: float = 15.0) -> dict:
+    """The CPU oracle (reference arithmetic, pool decomposition) on this host, bounded."""
+    o = setup_oracle(wl)
+    threads = host_threads()
+    o.step_forces(1, threads=threads)      # warm caches / page in
+    t0 = time.perf_counter()
+    o.step_forces(1, threads=threads)
+    t1 = time.perf_counter() - t0
+    steps = max(1, min(200, int(budget_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    o.step_forces(steps, threads=threads)
+    dt = time.perf_counter() - t0
+    n = wl["nx"] * wl["ny"] * wl["nz"]
+    o.close()
+    return {"value": n * steps / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": f"{steps} full steps of the {wl['nx']}x{wl['ny']}x{wl['nz']} workload "
+                      f"(oracle: float64 arithmetic, float32 storage, OpenMP z-slabs as "
+                      f"js/pool.js), {cpu_model()}"}
+
+
+# ---------------------------------------------------------------------------- arms
+def run_wt(args) -> None:
+    import torch
+    dist = Dist()
+    dist.init()
+    wl = WORKLOADS[args.workload]
+    n = wl["nx"] * wl["ny"] * wl["nz"]
+    K, W = args.steps, args.warmup
+    peak, peak_kind = measured_peaks()
+
+    sim = setup_gpu(wl, "f32", "fast")
+    sim.step_forces(W)
+    clocks = ClockSampler(torch.cuda.current_device()).start() if dist.rank == 0 else None
+    ms, launches = timed_steps(sim, K, dist)
+    clk = clocks.stop() if clocks else None
+    ms_max = dist.max(ms)
+    value = dist.world * n * K / (ms_max * 1e-3) / 1e6
+
+    # public per-step path (host buffers, one sync per step)
+    sim.step_forces(W)
+    ke = max(W, K // 4)
+    e2e_ms = dist.max(e2e_steps(sim, ke, dist))
+    from windtunnel_b200._lib import wt_params
+    import ctypes
+    h2d = ctypes.sizeof(wt_params)
+    d2h = 3 * 8 + 4
+    e2e_val = dist.world * n * ke / (e2e_ms * 1e-3) / 1e6
+    sim.close()
+
+    # half-deviation storage on the same workload
+    s16 = setup_gpu(wl, "f16dev", "fast")
+    s16.step_forces(W)
+    ms16, _ = timed_steps(s16, K, dist)
+    ms16 = dist.max(ms16)
+    v16 = dist.world * n * K / (ms16 * 1e-3) / 1e6
+    s16.close()
+
+    achieved = BYTES_PER_CELL["f32"] * n * K / (ms * 1e-3) / 1e9
+    traffic = profiled_traffic(f"k_step_f32_fast_{wl['nx']}x{wl['ny']}x{wl['nz']}")
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": dist.world,
+        "steps": K, "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl["name"], "lattice": [wl["nx"], wl["ny"], wl["nz"]],
+                   "cells": n, "storage": "f32", "collision": "float32 (WT_MATH_FAST)",
+                   "tau": wl["tau"], "u0": wl["u0"], "les_cs": wl["csm"], "trt_lambda": wl["lam"],
+                   "side_bc": wl["side_bc"],
+                   "l2": "inputs larger than L2: two 318.8 MB population buffers per replica",
+                   "parallelism": f"replicas{dist.world}" if dist.world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_source": peak_kind,
+                     "bytes_per_cell": BYTES_PER_CELL["f32"],
+                     "note": "achieved = 152 B x cells x steps / event time of the K-step call"},
+        "e2e": {"value": round(e2e_val, 1), "unit": "MLUPS", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": ke,
+                "path": "LBM.step() per step: wt_set_params + wt_step(1) + force to host"},
+        "gpu_launches": launches,
+        "fp16dev": {"value": round(v16, 1), "unit": "MLUPS", "ms_per_step": ms16 / K,
+                    "over_fp32": round(v16 / value, 3),
+                    "roofline_frac": round(BYTES_PER_CELL["f16dev"] * n * K / (ms16 * 1e-3) /
+                                           1e9 / peak, 4)},
+        "clocks": clk,
+    }
+    if args.accuracy and dist.rank == 0:
+        line["accuracy"] = accuracy_study(wl)
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wl)
+    dist.barrier()
+    dist.close()
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args) -> None:
+    """The reference's CPU path (the oracle port) on this host's cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wl = WORKLOADS[args.workload]
+    K, W = args.steps, args.warmup
+    threads = host_threads()
+    o = setup_oracle(wl)
+    nx, ny, nz = wl["nx"], wl["ny"], wl["nz"]
+    # size each timed step as a z-slab sample so the whole run stays within the budget
+    t0 = time.perf_counter()
+    o.step_sample(1, nz - 1, threads)
+    t_full = time.perf_counter() - t0
+    budget = args.reference_budget
+    planes = nz - 2
+    if (K + W) * t_full > budget:
+        planes = max(threads, int((nz - 2) * budget / ((K + W) * t_full)))
+        planes = min(planes, nz - 2)
+    z0, z1 = 1, 1 + planes
+    for _ in range(W):
+        o.step_sample(z0, z1, threads)
+    cells = 0
+    t0 = time.perf_counter()
+    for _ in range(K):
+        cells += o.step_sample(z0, z1, threads)
+    dt = time.perf_counter() - t0
+    value = cells / dt / 1e6
+    sample = (f"each step: interior z-planes [{z0},{z1}) of the {nx}x{ny}x{nz} lattice "
+              f"({nx * ny * planes} cells, stepSlab + boundaries), {threads} threads, "
+              f"{cpu_model()}")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "MLUPS",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": K, "warmup": W,
+        "ms_per_step": dt * 1e3 / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["name"], "lattice": [nx, ny, nz], "storage": "f32"},
+        "cpu_baseline": {"value": round(value, 2), "unit": "MLUPS", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "the reference is browser JavaScript (js/lbm.js); no JS engine exists on this "
+                "host, so its arithmetic is timed through the C restatement in oracle/"}),
+        flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", choices=["wt", "reference"], default="wt")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="channel256")
+    ap.add_argument("--no-accuracy", dest="accuracy", action="store_false")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-budget", type=float, default=90.0,
+                    help="seconds of timed CPU work for --impl reference")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_wt(args)
+
+
+if __name__ == "__main__":
+    main()

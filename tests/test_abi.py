@@ -1,0 +1,65 @@
+"""The C ABI: libwt.so loads and exports every entry point include/wt.h declares.
+
+No compute call is made here (these run without a GPU).
+"""
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "wt.h"
+
+
+def declared_functions(header: Path) -> list[str]:
+    text = header.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(wt_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions(HEADER)
+    for required in ("wt_create", "wt_destroy", "wt_step", "wt_voxelize_mask", "wt_voxelize_grid",
+                     "wt_get_fields", "wt_get_populations", "wt_last_error", "wt_get_state",
+                     "wt_set_state", "wt_sample", "wt_is_solid", "wt_reset"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol(wt_lib):
+    missing = [n for n in declared_functions(HEADER) if not hasattr(wt_lib, n)]
+    assert not missing, f"not exported: {missing}"
+
+
+def test_exports_are_c_symbols(wt_lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", wt_lib._name], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (wt_[a-z0-9_]+)\b", out))
+    assert set(declared_functions(HEADER)) <= exported
+
+
+def test_default_params_match_reference(wt_lib):
+    """js/lbm.js:106-111 defaults, without touching a device."""
+    from windtunnel_b200 import _lib
+    p = _lib.default_params()
+    assert p.u0 == 0.06 and p.tau == 0.5035 and p.les == 1 and p.csm == 0.14
+    assert p.trt == 1 and p.lambda_ == 0.25 and p.side_bc == 0 and p.math == 0
+
+
+def test_create_rejects_bad_dims_on_host(wt_lib):
+    """Argument checks happen before any CUDA call."""
+    from windtunnel_b200 import _lib
+    h = ctypes.c_void_p()
+    assert wt_lib.wt_create(2, 8, 8, 0, ctypes.byref(h)) == _lib.WT_ERR_ARG
+    assert b"at least 3" in wt_lib.wt_last_error(None)
+    assert wt_lib.wt_create(8, 8, 8, 7, ctypes.byref(h)) == _lib.WT_ERR_ARG
+    assert wt_lib.wt_create(8, 8, 8, 0, None) == _lib.WT_ERR_ARG
+    assert h.value is None
+
+
+def test_null_handle_is_an_argument_error(wt_lib):
+    from windtunnel_b200 import _lib
+    assert wt_lib.wt_step(None, 1, None) == _lib.WT_ERR_ARG
+    assert wt_lib.wt_reset(None) == _lib.WT_ERR_ARG
+    assert wt_lib.wt_destroy(None) == _lib.WT_OK

@@ -1,0 +1,707 @@
+// wt_api.cu — the extern "C" entry points of libwt.so (include/wt.h):
+// handle lifetime, parameters, voxelize, the batched step and the getters.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "wt_internal.h"
+
+namespace {
+
+thread_local std::string g_create_error;
+
+constexpr int kChunk = 32;         // steps whose force partials are reduced together
+constexpr uint32_t kStateMagic = 0x57545354u;  // "WTST"
+
+int fail(wt_lattice* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int cuda_fail(wt_lattice* h, cudaError_t e, const char* what) {
+  return fail(h, WT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define WT_CUDA(h, call)                                      \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_fail((h), e_, #call);  \
+  } while (0)
+
+size_t elem_size(int storage) {
+  return storage == WT_STORE_F32 ? 4 : (storage == WT_STORE_F16DEV ? 2 : 8);
+}
+
+// ECMAScript ToInt32 on the host (the `| 0` of js/lbm.js:542).
+int js_toint32(double v) {
+  if (!std::isfinite(v)) return 0;
+  if (v > -2147483649.0 && v < 2147483648.0) return (int)v;
+  double m = fmod(trunc(v), 4294967296.0);
+  if (m < 0) m += 4294967296.0;
+  return (int)(uint32_t)m;
+}
+
+int clamp_int(double v) {
+  if (v > 2147483647.0) return 2147483647;
+  if (v < -2147483647.0) return -2147483647;
+  return (int)v;
+}
+
+void voxel_range(int nx, int ny, int nz, const double box[6], int rg[6]) {
+  rg[0] = clamp_int(fmax(1, floor(box[0])));
+  rg[1] = clamp_int(fmin(nx - 2, ceil(box[3])));
+  rg[2] = clamp_int(fmax(1, floor(box[1])));
+  rg[3] = clamp_int(fmin(ny - 2, ceil(box[4])));
+  rg[4] = clamp_int(fmax(1, floor(box[2])));
+  rg[5] = clamp_int(fmin(nz - 2, ceil(box[5])));
+}
+
+long long range_cells(const int rg[6]) {
+  const long long ex = rg[1] >= rg[0] ? rg[1] - rg[0] + 1 : 0;
+  const long long ey = rg[3] >= rg[2] ? rg[3] - rg[2] + 1 : 0;
+  const long long ez = rg[5] >= rg[4] ? rg[5] - rg[4] + 1 : 0;
+  return ex * ey * ez;
+}
+
+void free_all(wt_lattice* h) {
+  void* dev[] = {h->buf[0], h->buf[1], h->flags, h->ux, h->uy, h->uz, h->rho, h->uwx, h->uwy,
+                 h->uwz, h->part, h->forces_dev, h->err_dev, h->col, h->plan, h->low,
+                 h->counters};
+  for (void* p : dev)
+    if (p) cudaFree(p);
+  if (h->forces_host) cudaFreeHost(h->forces_host);
+  if (h->err_host) cudaFreeHost(h->err_host);
+  if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+int check_params(const wt_params* p) {
+  if (!std::isfinite(p->u0) || !std::isfinite(p->tau) || !(p->tau > 0.5)) return WT_ERR_ARG;
+  if (!std::isfinite(p->csm) || !std::isfinite(p->lambda)) return WT_ERR_ARG;
+  if (p->trt && !(p->lambda > 0)) return WT_ERR_ARG;
+  if (p->side_bc != WT_SIDE_EQ && p->side_bc != WT_SIDE_FREESLIP) return WT_ERR_ARG;
+  if (p->math != WT_MATH_FAST && p->math != WT_MATH_EXACT) return WT_ERR_ARG;
+  if (p->reserved != 0) return WT_ERR_ARG;
+  return WT_OK;
+}
+
+int grow_forces(wt_lattice* h, int nsteps) {
+  if (nsteps <= h->forces_cap) return WT_OK;
+  int cap = std::max(nsteps, 2 * h->forces_cap);
+  if (h->forces_dev) cudaFree(h->forces_dev);
+  if (h->forces_host) cudaFreeHost(h->forces_host);
+  h->forces_dev = nullptr;
+  h->forces_host = nullptr;
+  h->forces_cap = 0;
+  if (cudaMalloc(&h->forces_dev, sizeof(double) * 3 * (size_t)cap) != cudaSuccess)
+    return fail(h, WT_ERR_OOM, "cannot allocate the device force series");
+  if (cudaMallocHost(&h->forces_host, sizeof(double) * 3 * (size_t)cap) != cudaSuccess)
+    return fail(h, WT_ERR_OOM, "cannot allocate the pinned force series");
+  h->forces_cap = cap;
+  return WT_OK;
+}
+
+template <class S>
+S to_store(double v);
+template <>
+float to_store<float>(double v) { return (float)v; }
+template <>
+double to_store<double>(double v) { return v; }
+template <>
+__half to_store<__half>(double v) { return __double2half(v * WT_F16_SCALE); }
+
+template <class S>
+wt::StepArgs<S> make_args(wt_lattice* h) {
+  wt::StepArgs<S> a{};
+  a.flags = h->flags;
+  a.ux = h->ux; a.uy = h->uy; a.uz = h->uz; a.rho = h->rho;
+  a.uwx = h->uwx; a.uwy = h->uwy; a.uwz = h->uwz;
+  a.err = h->err_dev;
+  a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
+  a.n = h->n;
+  a.nxy = (long long)h->nx * h->ny;
+  const wt_params& p = h->p;
+  a.tau0 = p.tau;
+  a.omega0 = 1 / p.tau;
+  a.omm0 = p.trt ? 1 / (0.5 + p.lambda / (p.tau - 0.5)) : a.omega0;
+  a.cs2 = p.csm * p.csm;
+  a.lam = p.lambda;
+  a.les_c = 72 * a.cs2;
+  a.les = p.les ? 1 : 0;
+  a.trt = p.trt ? 1 : 0;
+  a.mov = p.moving_walls ? 1 : 0;
+  a.freeslip = p.side_bc == WT_SIDE_FREESLIP ? 1 : 0;
+  double eq[19];
+  wt::eq_u0_table(p.u0, eq);
+  for (int q = 0; q < 19; q++) a.eq[q] = to_store<S>(eq[q]);
+  a.u0f = (float)p.u0;
+  return a;
+}
+
+template <class S, class L>
+void run_steps(wt_lattice* h, int nsteps, L launch) {
+  wt::StepArgs<S> a = make_args<S>(h);
+  const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
+  for (int done = 0; done < nsteps;) {
+    const int chunk = std::min(kChunk, nsteps - done);
+    for (int s = 0; s < chunk; s++) {
+      a.F = (const S*)h->buf[h->parity];
+      a.G = (S*)h->buf[h->parity ^ 1];
+      a.part = h->part + (size_t)s * h->nblocks * 3;
+      a.write_fields = (done + s == nsteps - 1) ? 1 : 0;
+      launch(a, grid, h->stream);
+      h->launches++;
+      h->parity ^= 1;
+    }
+    wt::launch_force_reduce(h->part, h->nblocks, chunk, h->forces_dev + 3 * (size_t)done,
+                            h->stream);
+    h->launches++;
+    done += chunk;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void wt_default_params(wt_params* p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->u0 = 0.06;
+  p->tau = 0.5035;
+  p->les = 1;
+  p->trt = 1;
+  p->csm = 0.14;
+  p->lambda = 1.0 / 4;
+  p->moving_walls = 0;
+  p->side_bc = WT_SIDE_EQ;
+  p->math = WT_MATH_FAST;
+}
+
+const char* wt_last_error(const wt_lattice* h) {
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
+  g_create_error.clear();
+  if (!out) { g_create_error = "out is NULL"; return WT_ERR_ARG; }
+  *out = nullptr;
+  if (nx < 3 || ny < 3 || nz < 3) {
+    g_create_error = "lattice dims must be at least 3 in every direction";
+    return WT_ERR_ARG;
+  }
+  if (ny > 65535 || nz > 65535) {
+    g_create_error = "ny and nz must not exceed 65535";
+    return WT_ERR_ARG;
+  }
+  if (storage != WT_STORE_F32 && storage != WT_STORE_F16DEV && storage != WT_STORE_F64) {
+    g_create_error = "unknown storage format";
+    return WT_ERR_ARG;
+  }
+  const long long n = (long long)nx * ny * nz;
+  if (n > (1LL << 40) / 19) {
+    g_create_error = "lattice too large";
+    return WT_ERR_ARG;
+  }
+  wt_lattice* h = new wt_lattice();
+  h->nx = nx; h->ny = ny; h->nz = nz; h->n = n; h->storage = storage;
+  h->elem = elem_size(storage);
+  wt_default_params(&h->p);
+  h->stats.frontal_area = 1;
+  cudaGetDevice(&h->device);
+  const dim3 grid = wt::step_grid(nx, ny, nz);
+  h->nblocks = grid.x * grid.y * grid.z;
+  h->part_steps = kChunk;
+  const size_t pop = (size_t)n * 19 * h->elem;
+  bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaMalloc(&h->buf[0], pop) == cudaSuccess;
+  ok = ok && cudaMalloc(&h->buf[1], pop) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->flags, (size_t)n) == cudaSuccess;
+  float** fl[] = {&h->ux, &h->uy, &h->uz, &h->rho, &h->uwx, &h->uwy, &h->uwz};
+  for (float** p : fl) ok = ok && cudaMalloc((void**)p, sizeof(float) * (size_t)n) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->part, sizeof(double) * 3 * (size_t)h->nblocks * kChunk) ==
+                 cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->err_dev, sizeof(unsigned)) == cudaSuccess;
+  ok = ok && cudaMallocHost((void**)&h->err_host, sizeof(unsigned)) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->col, (size_t)ny * nz) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->plan, (size_t)nx * nz) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->low, sizeof(int) * (size_t)nx * nz) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->counters, sizeof(int) * 2) == cudaSuccess;
+  ok = ok && grow_forces(h, 64) == WT_OK;
+  if (!ok) {
+    cudaGetLastError();
+    free_all(h);
+    delete h;
+    g_create_error = "device allocation failed for a " + std::to_string(nx) + "x" +
+                     std::to_string(ny) + "x" + std::to_string(nz) + " lattice";
+    return WT_ERR_OOM;
+  }
+  cudaMemsetAsync(h->flags, 0, (size_t)n, h->stream);
+  for (float* p : {h->uwx, h->uwy, h->uwz}) cudaMemsetAsync(p, 0, sizeof(float) * n, h->stream);
+  wt::launch_init(h, 0, 0, 0);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_create_error = std::string("initialisation failed: ") + cudaGetErrorString(e);
+    free_all(h);
+    delete h;
+    return WT_ERR_CUDA;
+  }
+  *out = h;
+  return WT_OK;
+}
+
+int wt_destroy(wt_lattice* h) {
+  if (!h) return WT_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return WT_OK;
+}
+
+int wt_get_dims(const wt_lattice* h, int* nx, int* ny, int* nz, int* storage) {
+  if (!h) return WT_ERR_ARG;
+  if (nx) *nx = h->nx;
+  if (ny) *ny = h->ny;
+  if (nz) *nz = h->nz;
+  if (storage) *storage = h->storage;
+  return WT_OK;
+}
+
+int wt_set_params(wt_lattice* h, const wt_params* p) {
+  if (!h) return WT_ERR_ARG;
+  if (!p) return fail(h, WT_ERR_ARG, "params is NULL");
+  const int c = check_params(p);
+  if (c != WT_OK)
+    return fail(h, c, "invalid parameters (need finite u0/csm/lambda, tau > 0.5, lambda > 0 "
+                      "with trt, known side_bc and math, reserved = 0)");
+  if (h->storage == WT_STORE_F16DEV && p->math == WT_MATH_EXACT)
+    return fail(h, WT_ERR_UNSUPPORTED, "half storage runs the float32 collision only");
+  h->p = *p;
+  return WT_OK;
+}
+
+int wt_get_params(const wt_lattice* h, wt_params* p) {
+  if (!h || !p) return WT_ERR_ARG;
+  *p = h->p;
+  return WT_OK;
+}
+
+int wt_reset(wt_lattice* h) {
+  if (!h) return WT_ERR_ARG;
+  wt::launch_init(h, 0, 0, 0);
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  WT_CUDA(h, cudaGetLastError());
+  h->steps = 0;
+  h->force[0] = h->force[1] = h->force[2] = 0;
+  return WT_OK;
+}
+
+int wt_init_eq_noise(wt_lattice* h, uint64_t seed, double amp) {
+  if (!h) return WT_ERR_ARG;
+  if (!std::isfinite(amp)) return fail(h, WT_ERR_ARG, "amp must be finite");
+  wt::launch_init(h, 1, seed, amp);
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  WT_CUDA(h, cudaGetLastError());
+  h->steps = 0;
+  h->force[0] = h->force[1] = h->force[2] = 0;
+  return WT_OK;
+}
+
+int wt_voxel_range(const wt_lattice* h, const double box[6], int range[6]) {
+  if (!h || !box || !range) return WT_ERR_ARG;
+  voxel_range(h->nx, h->ny, h->nz, box, range);
+  return WT_OK;
+}
+
+namespace {
+
+// Shared tail of both voxelize forms: statistics and near flags.
+int voxelize_finish(wt_lattice* h, int ground, double road_vel) {
+  std::vector<uint8_t> col((size_t)h->ny * h->nz), plan((size_t)h->nx * h->nz);
+  std::vector<int> low((size_t)h->nx * h->nz);
+  int counters[2] = {0, 0};
+  WT_CUDA(h, cudaMemcpyAsync(col.data(), h->col, col.size(), cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaMemcpyAsync(plan.data(), h->plan, plan.size(), cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaMemcpyAsync(low.data(), h->low, sizeof(int) * low.size(), cudaMemcpyDeviceToHost,
+                             h->stream));
+  WT_CUDA(h, cudaMemcpyAsync(counters, h->counters, sizeof(counters), cudaMemcpyDeviceToHost,
+                             h->stream));
+  wt::launch_near(h);
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  WT_CUDA(h, cudaGetLastError());
+  // js/lbm.js:247-264
+  long long a = 0, pa = 0;
+  for (uint8_t v : col) a += v;
+  for (uint8_t v : plan) pa += v;
+  std::vector<int> gaps;
+  for (size_t k = 0; k < plan.size(); k++) {
+    if (plan[k] && low[k] < 32767) {
+      const int g = low[k] - 1;
+      if (g > 0) gaps.push_back(g);
+    }
+  }
+  std::sort(gaps.begin(), gaps.end());
+  h->stats.frontal_area = (int)std::max<long long>(1, a);
+  h->stats.planform_area = (int)std::max<long long>(1, pa);
+  h->stats.solid_cells = counters[0];
+  h->stats.ride_height = gaps.empty() ? 0 : gaps[gaps.size() >> 1];
+  h->stats.ground = ground ? 1 : 0;
+  h->p.moving_walls = (road_vel != 0 || counters[1]) ? 1 : 0;
+  h->stats.moving_walls = h->p.moving_walls;
+  return WT_OK;
+}
+
+int voxelize_start(wt_lattice* h, int ground, double road_vel) {
+  wt::launch_clear_obj(h);
+  wt::launch_floor(h, ground, road_vel);
+  std::vector<int> low((size_t)h->nx * h->nz, 32767);
+  WT_CUDA(h, cudaMemsetAsync(h->col, 0, (size_t)h->ny * h->nz, h->stream));
+  WT_CUDA(h, cudaMemsetAsync(h->plan, 0, (size_t)h->nx * h->nz, h->stream));
+  WT_CUDA(h, cudaMemcpyAsync(h->low, low.data(), sizeof(int) * low.size(), cudaMemcpyHostToDevice,
+                             h->stream));
+  WT_CUDA(h, cudaMemsetAsync(h->counters, 0, sizeof(int) * 2, h->stream));
+  // the host vector must outlive the async copy
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+}  // namespace
+
+int wt_voxelize_mask(wt_lattice* h, const double box[6], const uint8_t* inside, size_t inside_len,
+                     const uint8_t* wall_set, const double* wall_vel, int ground, double road_vel) {
+  if (!h) return WT_ERR_ARG;
+  if (!box) return fail(h, WT_ERR_ARG, "box is NULL");
+  if (!std::isfinite(road_vel)) return fail(h, WT_ERR_ARG, "road_vel must be finite");
+  int rg[6];
+  voxel_range(h->nx, h->ny, h->nz, box, rg);
+  const long long cells = range_cells(rg);
+  if ((long long)inside_len != cells)
+    return fail(h, WT_ERR_ARG, "inside has " + std::to_string(inside_len) +
+                                   " entries; the scan range of box holds " +
+                                   std::to_string(cells));
+  if (cells > 0 && !inside) return fail(h, WT_ERR_ARG, "inside is NULL");
+  if (wall_set && !wall_vel) return fail(h, WT_ERR_ARG, "wall_set given without wall_vel");
+  int c = voxelize_start(h, ground, road_vel);
+  if (c != WT_OK) return c;
+  if (cells > 0) {
+    uint8_t* mask_dev = nullptr;
+    uint8_t* ws_dev = nullptr;
+    double* wv_dev = nullptr;
+    cudaError_t e = cudaMalloc(&mask_dev, (size_t)cells);
+    if (e == cudaSuccess && wall_set) e = cudaMalloc(&ws_dev, (size_t)cells);
+    if (e == cudaSuccess && wall_set) e = cudaMalloc(&wv_dev, sizeof(double) * 3 * (size_t)cells);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(mask_dev, inside, (size_t)cells, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && wall_set)
+      e = cudaMemcpyAsync(ws_dev, wall_set, (size_t)cells, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && wall_set)
+      e = cudaMemcpyAsync(wv_dev, wall_vel, sizeof(double) * 3 * (size_t)cells,
+                          cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) wt::launch_box_mask(h, rg, mask_dev, ws_dev, wv_dev);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (mask_dev) cudaFree(mask_dev);
+    if (ws_dev) cudaFree(ws_dev);
+    if (wv_dev) cudaFree(wv_dev);
+    if (e != cudaSuccess) return cuda_fail(h, e, "voxelize");
+  }
+  return voxelize_finish(h, ground, road_vel);
+}
+
+int wt_voxelize_grid(wt_lattice* h, const uint8_t* grid, int gnx, int gny, int gnz,
+                     const double gmin[3], double ginv, const double M[9], const double P[3],
+                     double scale, const double box[6], int ground, double road_vel) {
+  if (!h) return WT_ERR_ARG;
+  if (!grid || !gmin || !M || !P || !box) return fail(h, WT_ERR_ARG, "NULL argument");
+  if (gnx < 1 || gny < 1 || gnz < 1) return fail(h, WT_ERR_ARG, "grid dims must be positive");
+  if (!std::isfinite(road_vel)) return fail(h, WT_ERR_ARG, "road_vel must be finite");
+  int rg[6];
+  voxel_range(h->nx, h->ny, h->nz, box, rg);
+  const long long cells = range_cells(rg);
+  int c = voxelize_start(h, ground, road_vel);
+  if (c != WT_OK) return c;
+  if (cells > 0) {
+    const size_t gbytes = (size_t)gnx * gny * gnz;
+    uint8_t* grid_dev = nullptr;
+    cudaError_t e = cudaMalloc(&grid_dev, gbytes);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(grid_dev, grid, gbytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+      wt::launch_box_grid(h, rg, grid_dev, gnx, gny, gnz, gmin, ginv, M, P, scale);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (grid_dev) cudaFree(grid_dev);
+    if (e != cudaSuccess) return cuda_fail(h, e, "voxelize_grid");
+  }
+  return voxelize_finish(h, ground, road_vel);
+}
+
+int wt_get_body_stats(const wt_lattice* h, wt_body_stats* out) {
+  if (!h || !out) return WT_ERR_ARG;
+  *out = h->stats;
+  out->moving_walls = h->p.moving_walls;
+  return WT_OK;
+}
+
+int wt_step(wt_lattice* h, int nsteps, double* forces) {
+  if (!h) return WT_ERR_ARG;
+  if (nsteps < 0) return fail(h, WT_ERR_ARG, "nsteps must be >= 0");
+  if (nsteps == 0) return WT_OK;
+  int c = grow_forces(h, nsteps);
+  if (c != WT_OK) return c;
+  WT_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(unsigned), h->stream));
+  const bool exact = h->p.math == WT_MATH_EXACT;
+  switch (h->storage) {
+    case WT_STORE_F32:
+      if (exact) run_steps<float>(h, nsteps, wt::launch_step_f32_exact);
+      else run_steps<float>(h, nsteps, wt::launch_step_f32_fast);
+      break;
+    case WT_STORE_F16DEV:
+      run_steps<__half>(h, nsteps, wt::launch_step_f16_fast);
+      break;
+    default:
+      run_steps<double>(h, nsteps, wt::launch_step_f64_exact);
+      break;
+  }
+  WT_CUDA(h, cudaGetLastError());
+  WT_CUDA(h, cudaMemcpyAsync(h->forces_host, h->forces_dev, sizeof(double) * 3 * (size_t)nsteps,
+                             cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaMemcpyAsync(h->err_host, h->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             h->stream));
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->steps += nsteps;
+  const double* last = h->forces_host + 3 * (size_t)(nsteps - 1);
+  h->force[0] = last[0]; h->force[1] = last[1]; h->force[2] = last[2];
+  if (forces) memcpy(forces, h->forces_host, sizeof(double) * 3 * (size_t)nsteps);
+  if (*h->err_host)
+    return fail(h, WT_ERR_DIVERGED, "a step produced a non-finite or non-positive density");
+  return WT_OK;
+}
+
+int wt_get_force(const wt_lattice* h, double out[3]) {
+  if (!h || !out) return WT_ERR_ARG;
+  out[0] = h->force[0]; out[1] = h->force[1]; out[2] = h->force[2];
+  return WT_OK;
+}
+
+int wt_get_steps(const wt_lattice* h, int64_t* steps, int* parity) {
+  if (!h) return WT_ERR_ARG;
+  if (steps) *steps = h->steps;
+  if (parity) *parity = h->parity;
+  return WT_OK;
+}
+
+int wt_get_fields(wt_lattice* h, float* ux, float* uy, float* uz, float* rho) {
+  if (!h) return WT_ERR_ARG;
+  const size_t b = sizeof(float) * (size_t)h->n;
+  if (ux) WT_CUDA(h, cudaMemcpyAsync(ux, h->ux, b, cudaMemcpyDeviceToHost, h->stream));
+  if (uy) WT_CUDA(h, cudaMemcpyAsync(uy, h->uy, b, cudaMemcpyDeviceToHost, h->stream));
+  if (uz) WT_CUDA(h, cudaMemcpyAsync(uz, h->uz, b, cudaMemcpyDeviceToHost, h->stream));
+  if (rho) WT_CUDA(h, cudaMemcpyAsync(rho, h->rho, b, cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_get_solid(wt_lattice* h, uint8_t* out) {
+  if (!h || !out) return WT_ERR_ARG;
+  std::vector<uint8_t> fl((size_t)h->n);
+  WT_CUDA(h, cudaMemcpyAsync(fl.data(), h->flags, fl.size(), cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (size_t i = 0; i < fl.size(); i++) out[i] = fl[i] & wt::FLAG_SOLID_MASK;
+  return WT_OK;
+}
+
+int wt_get_near(wt_lattice* h, uint8_t* out) {
+  if (!h || !out) return WT_ERR_ARG;
+  std::vector<uint8_t> fl((size_t)h->n);
+  WT_CUDA(h, cudaMemcpyAsync(fl.data(), h->flags, fl.size(), cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (size_t i = 0; i < fl.size(); i++) out[i] = (fl[i] & wt::FLAG_NEAR) ? 1 : 0;
+  return WT_OK;
+}
+
+int wt_get_populations(wt_lattice* h, int which, int dtype, void* out, size_t bytes) {
+  if (!h) return WT_ERR_ARG;
+  if (!out) return fail(h, WT_ERR_ARG, "out is NULL");
+  if (which != WT_BUF_F && which != WT_BUF_G) return fail(h, WT_ERR_ARG, "which must be F or G");
+  const bool raw = dtype == h->storage;
+  if (!raw && dtype != WT_STORE_F32 && dtype != WT_STORE_F64)
+    return fail(h, WT_ERR_ARG, "dtype must be F32, F64 or the handle's storage");
+  const long long count = 19LL * h->n;
+  const size_t want = (size_t)count * elem_size(dtype);
+  if (bytes != want)
+    return fail(h, WT_ERR_ARG, "bytes must be " + std::to_string(want));
+  const void* src = h->buf[h->parity ^ (which == WT_BUF_G ? 1 : 0)];
+  if (raw) {
+    WT_CUDA(h, cudaMemcpyAsync(out, src, want, cudaMemcpyDeviceToHost, h->stream));
+    WT_CUDA(h, cudaStreamSynchronize(h->stream));
+    return WT_OK;
+  }
+  void* tmp = nullptr;
+  if (cudaMalloc(&tmp, want) != cudaSuccess) return fail(h, WT_ERR_OOM, "conversion buffer");
+  wt::launch_convert(src, h->storage, tmp, dtype, count, h->stream);
+  h->launches++;
+  cudaError_t e = cudaMemcpyAsync(out, tmp, want, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(h, e, "get_populations");
+  return WT_OK;
+}
+
+int wt_set_populations(wt_lattice* h, int which, int dtype, const void* in, size_t bytes) {
+  if (!h) return WT_ERR_ARG;
+  if (!in) return fail(h, WT_ERR_ARG, "in is NULL");
+  if (which != WT_BUF_F && which != WT_BUF_G) return fail(h, WT_ERR_ARG, "which must be F or G");
+  const bool raw = dtype == h->storage;
+  if (!raw && dtype != WT_STORE_F32 && dtype != WT_STORE_F64)
+    return fail(h, WT_ERR_ARG, "dtype must be F32, F64 or the handle's storage");
+  const long long count = 19LL * h->n;
+  const size_t want = (size_t)count * elem_size(dtype);
+  if (bytes != want)
+    return fail(h, WT_ERR_ARG, "bytes must be " + std::to_string(want));
+  void* dst = h->buf[h->parity ^ (which == WT_BUF_G ? 1 : 0)];
+  if (raw) {
+    WT_CUDA(h, cudaMemcpyAsync(dst, in, want, cudaMemcpyHostToDevice, h->stream));
+    WT_CUDA(h, cudaStreamSynchronize(h->stream));
+    return WT_OK;
+  }
+  void* tmp = nullptr;
+  if (cudaMalloc(&tmp, want) != cudaSuccess) return fail(h, WT_ERR_OOM, "conversion buffer");
+  cudaError_t e = cudaMemcpyAsync(tmp, in, want, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    wt::launch_convert_in(tmp, dtype, dst, h->storage, count, h->stream);
+    h->launches++;
+    e = cudaStreamSynchronize(h->stream);
+  }
+  cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(h, e, "set_populations");
+  return WT_OK;
+}
+
+namespace {
+struct StateHeader {
+  uint32_t magic;
+  int32_t nx, ny, nz, storage, parity;
+  int64_t steps;
+  double force[3];
+  wt_params params;
+  wt_body_stats stats;
+};
+
+size_t state_bytes(const wt_lattice* h) {
+  return sizeof(StateHeader) + 2 * (size_t)h->n * 19 * h->elem + (size_t)h->n +
+         7 * sizeof(float) * (size_t)h->n;
+}
+}  // namespace
+
+int wt_state_size(const wt_lattice* h, size_t* bytes) {
+  if (!h || !bytes) return WT_ERR_ARG;
+  *bytes = state_bytes(h);
+  return WT_OK;
+}
+
+int wt_get_state(wt_lattice* h, void* out, size_t bytes) {
+  if (!h || !out) return WT_ERR_ARG;
+  if (bytes != state_bytes(h)) return fail(h, WT_ERR_ARG, "state buffer has the wrong size");
+  StateHeader hd{};
+  hd.magic = kStateMagic;
+  hd.nx = h->nx; hd.ny = h->ny; hd.nz = h->nz; hd.storage = h->storage; hd.parity = h->parity;
+  hd.steps = h->steps;
+  memcpy(hd.force, h->force, sizeof(hd.force));
+  hd.params = h->p;
+  hd.stats = h->stats;
+  char* o = (char*)out;
+  memcpy(o, &hd, sizeof(hd));
+  o += sizeof(hd);
+  const size_t pop = (size_t)h->n * 19 * h->elem, fb = sizeof(float) * (size_t)h->n;
+  WT_CUDA(h, cudaMemcpyAsync(o, h->buf[0], pop, cudaMemcpyDeviceToHost, h->stream)); o += pop;
+  WT_CUDA(h, cudaMemcpyAsync(o, h->buf[1], pop, cudaMemcpyDeviceToHost, h->stream)); o += pop;
+  WT_CUDA(h, cudaMemcpyAsync(o, h->flags, (size_t)h->n, cudaMemcpyDeviceToHost, h->stream));
+  o += h->n;
+  for (float* p : {h->ux, h->uy, h->uz, h->rho, h->uwx, h->uwy, h->uwz}) {
+    WT_CUDA(h, cudaMemcpyAsync(o, p, fb, cudaMemcpyDeviceToHost, h->stream));
+    o += fb;
+  }
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_set_state(wt_lattice* h, const void* in, size_t bytes) {
+  if (!h || !in) return WT_ERR_ARG;
+  if (bytes != state_bytes(h)) return fail(h, WT_ERR_ARG, "state buffer has the wrong size");
+  StateHeader hd;
+  memcpy(&hd, in, sizeof(hd));
+  if (hd.magic != kStateMagic || hd.nx != h->nx || hd.ny != h->ny || hd.nz != h->nz ||
+      hd.storage != h->storage)
+    return fail(h, WT_ERR_ARG, "state was taken from a different lattice");
+  if (check_params(&hd.params) != WT_OK) return fail(h, WT_ERR_ARG, "state holds invalid params");
+  const char* o = (const char*)in + sizeof(hd);
+  const size_t pop = (size_t)h->n * 19 * h->elem, fb = sizeof(float) * (size_t)h->n;
+  WT_CUDA(h, cudaMemcpyAsync(h->buf[0], o, pop, cudaMemcpyHostToDevice, h->stream)); o += pop;
+  WT_CUDA(h, cudaMemcpyAsync(h->buf[1], o, pop, cudaMemcpyHostToDevice, h->stream)); o += pop;
+  WT_CUDA(h, cudaMemcpyAsync(h->flags, o, (size_t)h->n, cudaMemcpyHostToDevice, h->stream));
+  o += h->n;
+  for (float* p : {h->ux, h->uy, h->uz, h->rho, h->uwx, h->uwy, h->uwz}) {
+    WT_CUDA(h, cudaMemcpyAsync(p, o, fb, cudaMemcpyHostToDevice, h->stream));
+    o += fb;
+  }
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->parity = hd.parity & 1;
+  h->steps = hd.steps;
+  memcpy(h->force, hd.force, sizeof(hd.force));
+  h->p = hd.params;
+  h->stats = hd.stats;
+  return WT_OK;
+}
+
+int wt_sample(wt_lattice* h, const double* xyz, int npts, double* out) {
+  if (!h) return WT_ERR_ARG;
+  if (npts < 0 || (npts > 0 && (!xyz || !out))) return fail(h, WT_ERR_ARG, "bad points");
+  if (npts == 0) return WT_OK;
+  double* d = nullptr;
+  if (cudaMalloc(&d, sizeof(double) * 6 * (size_t)npts) != cudaSuccess)
+    return fail(h, WT_ERR_OOM, "sample buffer");
+  cudaError_t e = cudaMemcpyAsync(d, xyz, sizeof(double) * 3 * (size_t)npts,
+                                  cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    wt::launch_sample(h, d, npts, d + 3 * (size_t)npts);
+    e = cudaMemcpyAsync(out, d + 3 * (size_t)npts, sizeof(double) * 3 * (size_t)npts,
+                        cudaMemcpyDeviceToHost, h->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(h, e, "sample");
+  return WT_OK;
+}
+
+int wt_is_solid(wt_lattice* h, double x, double y, double z, int* out) {
+  if (!h || !out) return WT_ERR_ARG;
+  const int xi = js_toint32(x), yi = js_toint32(y), zi = js_toint32(z);
+  if (xi < 0 || yi < 0 || zi < 0 || xi >= h->nx || yi >= h->ny || zi >= h->nz) {
+    *out = 0;
+    return WT_OK;
+  }
+  uint8_t v = 0;
+  const long long i = xi + (long long)h->nx * (yi + (long long)h->ny * zi);
+  WT_CUDA(h, cudaMemcpyAsync(&v, h->flags + i, 1, cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  *out = (v & wt::FLAG_SOLID_MASK) != 0;
+  return WT_OK;
+}
+
+int wt_get_stream(const wt_lattice* h, void** stream) {
+  if (!h || !stream) return WT_ERR_ARG;
+  *stream = (void*)h->stream;
+  return WT_OK;
+}
+
+int wt_get_launch_count(const wt_lattice* h, int64_t* count) {
+  if (!h || !count) return WT_ERR_ARG;
+  *count = h->launches;
+  return WT_OK;
+}
+
+}  // extern "C"

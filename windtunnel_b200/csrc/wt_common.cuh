@@ -1,0 +1,120 @@
+// wt_common.cuh — D3Q19 lattice constants, storage formats and the
+// parameter blocks shared by every kernel of libwt.so.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/wt.h"
+
+namespace wt {
+
+constexpr int Q = 19;
+constexpr int FLAG_SOLID_MASK = 3;  // low two bits: WT_FLUID / WT_SOLID_OBJ / WT_SOLID_WALL
+constexpr int FLAG_NEAR = 4;        // bit 2: fluid interior cell with a solid neighbour
+
+// Direction set of js/lbm.js:29-33 (the order is part of the f-buffer layout).
+__host__ __device__ constexpr int ex(int q) {
+  constexpr int t[Q] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+  return t[q];
+}
+__host__ __device__ constexpr int ey(int q) {
+  constexpr int t[Q] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1};
+  return t[q];
+}
+__host__ __device__ constexpr int ez(int q) {
+  constexpr int t[Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1};
+  return t[q];
+}
+__host__ __device__ constexpr int opp(int q) {
+  constexpr int t[Q] = {0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17};
+  return t[q];
+}
+// Mirror images in y and in z (free-slip side planes).
+__host__ __device__ constexpr int mirror_y(int q) {
+  constexpr int t[Q] = {0, 1, 2, 4, 3, 5, 6, 10, 9, 8, 7, 11, 12, 13, 14, 18, 17, 16, 15};
+  return t[q];
+}
+__host__ __device__ constexpr int mirror_z(int q) {
+  constexpr int t[Q] = {0, 1, 2, 3, 4, 6, 5, 7, 8, 9, 10, 13, 14, 11, 12, 17, 18, 15, 16};
+  return t[q];
+}
+// Lattice weights (js/lbm.js:34-37), as the IEEE doubles 1/3, 1/18, 1/36.
+__host__ __device__ constexpr double wq(int q) {
+  return q == 0 ? 1.0 / 3 : (q <= 6 ? 1.0 / 18 : 1.0 / 36);
+}
+
+// ---- storage formats -------------------------------------------------------
+// Each trait converts between the stored deviation and the arithmetic type.
+template <class S>
+struct Store;
+
+template <>
+struct Store<float> {
+  static constexpr int kind = WT_STORE_F32;
+  __device__ __forceinline__ static float load_f(float v) { return v; }
+  __device__ __forceinline__ static double load_d(float v) { return (double)v; }
+  __device__ __forceinline__ static float from_f(float v) { return v; }
+  __device__ __forceinline__ static float from_d(double v) { return __double2float_rn(v); }
+};
+
+template <>
+struct Store<double> {
+  static constexpr int kind = WT_STORE_F64;
+  __device__ __forceinline__ static float load_f(double v) { return (float)v; }
+  __device__ __forceinline__ static double load_d(double v) { return v; }
+  __device__ __forceinline__ static double from_f(float v) { return (double)v; }
+  __device__ __forceinline__ static double from_d(double v) { return v; }
+};
+
+// Half-precision deviations, scaled by WT_F16_SCALE (a power of two, so the
+// scaling itself is exact).
+template <>
+struct Store<__half> {
+  static constexpr int kind = WT_STORE_F16DEV;
+  __device__ __forceinline__ static float load_f(__half v) {
+    return __half2float(v) * (float)(1.0 / WT_F16_SCALE);
+  }
+  __device__ __forceinline__ static double load_d(__half v) { return (double)load_f(v); }
+  __device__ __forceinline__ static __half from_f(float v) {
+    return __float2half_rn(v * (float)WT_F16_SCALE);
+  }
+  __device__ __forceinline__ static __half from_d(double v) {
+    return __double2half(v * WT_F16_SCALE);
+  }
+};
+
+// ---- per-launch parameter block of the fused step --------------------------
+template <class S>
+struct StepArgs {
+  const S* F;          // populations read (current f)
+  S* G;                // populations written (next f)
+  const uint8_t* flags;
+  float* ux;
+  float* uy;
+  float* uz;
+  float* rho;
+  const float* uwx;
+  const float* uwy;
+  const float* uwz;
+  double* part;        // this step's per-block force partials, 3 per block
+  unsigned* err;       // bit 0: non-finite / non-positive density seen
+  int nx, ny, nz;
+  long long n;         // nx*ny*nz
+  long long nxy;       // nx*ny
+  double tau0, omega0, omm0, cs2, lam;
+  double les_c;        // 72*cs2: the LES constant folded for the fast body
+  int les, trt, mov, freeslip, write_fields;
+  S eq[Q];             // equilibrium deviation at rho=1, u=(u0,0,0), rounded to S
+  float u0f;           // (float)u0 for the boundary-cell fields
+};
+
+// Block shape of the fused step: one thread per cell along x.
+constexpr int STEP_BX = 128;
+
+inline dim3 step_grid(int nx, int ny, int nz) {
+  return dim3((unsigned)((nx + STEP_BX - 1) / STEP_BX), (unsigned)ny, (unsigned)nz);
+}
+
+}  // namespace wt

@@ -1,0 +1,92 @@
+// wt_internal.h — the handle behind wt_lattice* and the kernel launchers
+// shared by the translation units of libwt.so.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/wt.h"
+#include "wt_common.cuh"
+
+struct wt_lattice {
+  int nx = 0, ny = 0, nz = 0, storage = 0;
+  long long n = 0;
+  int device = 0;
+  size_t elem = 4;               // bytes per stored population
+  cudaStream_t stream = nullptr;
+  void* buf[2] = {nullptr, nullptr};  // population buffers A and B (js/lbm.js:74-75)
+  int parity = 0;                // js/lbm.js:80: f = parity ? B : A
+  uint8_t* flags = nullptr;      // solid code (bits 0-1) | near bit (bit 2)
+  float* ux = nullptr;
+  float* uy = nullptr;
+  float* uz = nullptr;
+  float* rho = nullptr;
+  float* uwx = nullptr;          // wall velocities of solid cells (js/lbm.js:92-94)
+  float* uwy = nullptr;
+  float* uwz = nullptr;
+  // per-step force reduction
+  unsigned nblocks = 0;          // blocks of one step launch
+  int part_steps = 0;            // steps whose partials fit in `part`
+  double* part = nullptr;
+  double* forces_dev = nullptr;
+  double* forces_host = nullptr; // pinned
+  int forces_cap = 0;            // steps that fit in forces_dev / forces_host
+  unsigned* err_dev = nullptr;
+  unsigned* err_host = nullptr;  // pinned
+  // voxelize statistics scratch
+  uint8_t* col = nullptr;        // ny*nz frontal projection
+  uint8_t* plan = nullptr;       // nx*nz planform projection
+  int* low = nullptr;            // nx*nz lowest body cell per column
+  int* counters = nullptr;       // [0] body cells, [1] wall velocity seen
+  // host-side state
+  wt_params p{};
+  wt_body_stats stats{};
+  double force[3] = {0, 0, 0};
+  int64_t steps = 0;
+  int64_t launches = 0;
+  std::string err;
+};
+
+namespace wt {
+
+// Step launchers (one per storage x arithmetic pair that is provided).
+void launch_step_f32_fast(const StepArgs<float>& a, dim3 grid, cudaStream_t s);
+void launch_step_f16_fast(const StepArgs<__half>& a, dim3 grid, cudaStream_t s);
+void launch_step_f32_exact(const StepArgs<float>& a, dim3 grid, cudaStream_t s);
+void launch_step_f64_exact(const StepArgs<double>& a, dim3 grid, cudaStream_t s);
+
+// Deterministic per-step sum of the block partials: out[3*s..3*s+2].
+void launch_force_reduce(const double* part, unsigned nblocks, int nsteps, double* out,
+                         cudaStream_t s);
+
+// Equilibrium initialisation of both buffers and the fields:
+// mode 0 = reset(), mode 1 = reset() + seeded noise.
+void launch_init(wt_lattice* h, int mode, uint64_t seed, double amp);
+
+// voxelize pieces (js/lbm.js:197-214, :225-246, :268-282).
+void launch_clear_obj(wt_lattice* h);
+void launch_floor(wt_lattice* h, int ground, double road_vel);
+void launch_box_mask(wt_lattice* h, const int rg[6], const uint8_t* mask_dev,
+                     const uint8_t* wall_set_dev, const double* wall_vel_dev);
+void launch_box_grid(wt_lattice* h, const int rg[6], const uint8_t* grid_dev, int gnx, int gny,
+                     int gnz, const double gmin[3], double ginv, const double M[9],
+                     const double P[3], double scale);
+void launch_near(wt_lattice* h);
+
+// Population conversion to float32 / float64 deviations.
+void launch_convert(const void* src, int storage, void* dst, int dtype, long long count,
+                    cudaStream_t s);
+void launch_convert_in(const void* src, int dtype, void* dst, int storage, long long count,
+                       cudaStream_t s);
+
+// Trilinear velocity sample of js/lbm.js:515-539 for npts points.
+void launch_sample(wt_lattice* h, const double* xyz_dev, int npts, double* out_dev);
+
+// Equilibrium deviation at rho=1, u=(u0,0,0) per direction, in float64 with
+// the operation order of js/lbm.js:155-162.
+void eq_u0_table(double u0, double out[19]);
+
+}  // namespace wt

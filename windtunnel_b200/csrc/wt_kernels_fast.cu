@@ -1,0 +1,57 @@
+// wt_kernels_fast.cu — float32-arithmetic instantiations of the fused step
+// (float32 and half-deviation storage), plus the force reduction. Built with
+// the default multiply-add contraction.
+#include "wt_internal.h"
+#include "wt_step.cuh"
+
+namespace wt {
+
+void launch_step_f32_fast(const StepArgs<float>& a, dim3 grid, cudaStream_t s) {
+  k_step<float, false><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+void launch_step_f16_fast(const StepArgs<__half>& a, dim3 grid, cudaStream_t s) {
+  k_step<__half, false><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+// One block per step; each thread sums a fixed strided subset of the block
+// partials, then a fixed-shape tree combines them. The order never depends
+// on timing, so the force series is reproducible run to run.
+constexpr int RED_T = 256;
+
+__global__ void __launch_bounds__(RED_T) k_force_reduce(const double* __restrict__ part,
+                                                        unsigned nblocks,
+                                                        double* __restrict__ out) {
+  __shared__ double sm[3][RED_T];
+  const double* p = part + (size_t)blockIdx.x * nblocks * 3;
+  double ax = 0, ay = 0, az = 0;
+  for (unsigned b = threadIdx.x; b < nblocks; b += RED_T) {
+    ax += p[3 * (size_t)b];
+    ay += p[3 * (size_t)b + 1];
+    az += p[3 * (size_t)b + 2];
+  }
+  sm[0][threadIdx.x] = ax;
+  sm[1][threadIdx.x] = ay;
+  sm[2][threadIdx.x] = az;
+  __syncthreads();
+  for (int w = RED_T / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      sm[0][threadIdx.x] += sm[0][threadIdx.x + w];
+      sm[1][threadIdx.x] += sm[1][threadIdx.x + w];
+      sm[2][threadIdx.x] += sm[2][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[3 * (size_t)blockIdx.x] = sm[0][0];
+    out[3 * (size_t)blockIdx.x + 1] = sm[1][0];
+    out[3 * (size_t)blockIdx.x + 2] = sm[2][0];
+  }
+}
+
+void launch_force_reduce(const double* part, unsigned nblocks, int nsteps, double* out,
+                         cudaStream_t s) {
+  k_force_reduce<<<nsteps, RED_T, 0, s>>>(part, nblocks, out);
+}
+
+}  // namespace wt

@@ -1,0 +1,339 @@
+// wt_step.cuh — the fused D3Q19 step: pull-stream + halfway bounce-back +
+// momentum exchange + moments + equilibrium + Smagorinsky + TRT collide +
+// inlet / outlet / far-field boundaries, one launch per time step.
+//
+// Semantics follow one reference step, js/lbm.js:285-291: stepSlab over the
+// interior (js/lbm.js:303-466) followed by _boundaries (js/lbm.js:473-512).
+// The boundary pass is folded into the same launch by giving every cell a
+// category that reproduces the reference's write order:
+//   x == 0                         inlet: equilibrium (rho=1, u=(u0,0,0))
+//   z == 0 | z == nz-1 | y == ny-1 end planes / ceiling: equilibrium
+//   solid                          untouched (solid cells keep stale values)
+//   y == 0 (not solid)             floor: equilibrium
+//   otherwise                      fluid: collide and pull-stream
+// and the outlet column x = nx-1 receives a copy of whatever column nx-2
+// ends up holding; the thread of cell (nx-2, y, z) writes both cells, so the
+// copy needs neither a second pass nor a second computation.
+#pragma once
+
+#include <type_traits>
+
+#include "wt_common.cuh"
+
+namespace wt {
+
+// Load a stored deviation as the arithmetic type M.
+template <class M, class S>
+__device__ __forceinline__ M ld(S v) {
+  if constexpr (std::is_same<M, double>::value) return Store<S>::load_d(v);
+  else return Store<S>::load_f(v);
+}
+
+enum : int { CAT_NONE = 0, CAT_EQ = 1, CAT_KEEP = 2, CAT_FLUID = 3 };
+
+// Sum three doubles over the block in a fixed order and store them at
+// part[3*block]. Every thread of the block must call it.
+__device__ __forceinline__ void block_force_partial(double fx, double fy, double fz, bool link,
+                                                    double* part) {
+  __shared__ double red[3][STEP_BX / 32];
+  const unsigned blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (__syncthreads_or(link)) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      fx += __shfl_down_sync(0xffffffffu, fx, o);
+      fy += __shfl_down_sync(0xffffffffu, fy, o);
+      fz += __shfl_down_sync(0xffffffffu, fz, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = fx; red[1][w] = fy; red[2][w] = fz; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sx = 0, sy = 0, sz = 0;
+#pragma unroll
+      for (int k = 0; k < STEP_BX / 32; k++) { sx += red[0][k]; sy += red[1][k]; sz += red[2][k]; }
+      part[3 * (size_t)blk] = sx;
+      part[3 * (size_t)blk + 1] = sy;
+      part[3 * (size_t)blk + 2] = sz;
+    }
+  } else if (threadIdx.x == 0) {
+    part[3 * (size_t)blk] = 0;
+    part[3 * (size_t)blk + 1] = 0;
+    part[3 * (size_t)blk + 2] = 0;
+  }
+}
+
+// Gather for cells next to a solid (bounce-back + momentum exchange,
+// js/lbm.js:334-368) or next to a free-slip side plane (mirror gather).
+template <class S, class M>
+__device__ __forceinline__ void gather_special(const StepArgs<S>& a, long long i, int x, int y,
+                                               int z, bool shell, M (&f)[Q], double& Fx,
+                                               double& Fy, double& Fz, bool& link) {
+  const long long n = a.n;
+  const M rho_prev = (M)(a.mov ? a.rho[i] : 1.0f);
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    const long long off = ex(q) + (long long)ey(q) * a.nx + (long long)ez(q) * a.nxy;
+    const long long j = i - off;
+    const int s = q == 0 ? 0 : (a.flags[j] & FLAG_SOLID_MASK);
+    if (s) {
+      const M fd = ld<M>(a.F[opp(q) * n + i]);
+      M corr = 0;
+      if (a.mov) {
+        const M cu = (M)ex(q) * (M)a.uwx[j] + (M)ey(q) * (M)a.uwy[j] + (M)ez(q) * (M)a.uwz[j];
+        if (cu != (M)0) corr = (M)6 * (M)wq(q) * rho_prev * cu;
+      }
+      f[q] = fd + corr;
+      if (s == WT_SOLID_OBJ) {
+        const M d = (M)2 * fd + corr;
+        Fx -= (double)(d * (M)ex(q));
+        Fy -= (double)(d * (M)ey(q));
+        Fz -= (double)(d * (M)ez(q));
+        link = true;
+      }
+    } else {
+      long long src = q * n + i - off;
+      if (shell) {
+        int sx = x - ex(q), sy = y - ey(q), sz = z - ez(q), qq = q;
+        if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); }
+        if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); }
+        src = qq * n + sx + (long long)a.nx * sy + a.nxy * sz;
+      }
+      f[q] = ld<M>(a.F[src]);
+    }
+  }
+}
+
+template <class S>
+__device__ __forceinline__ void store_pair(S* G, long long idx, bool dup, S v) {
+  G[idx] = v;
+  if (dup) G[idx + 1] = v;
+}
+
+// Float32 collision, re-associated: opposite pairs are carried as half sums
+// and half differences, so moments, the equilibrium, the stress tensor of the
+// Smagorinsky model and the TRT update share their partial results. The
+// mathematics is that of js/lbm.js:377-460; only the rounding differs.
+template <class S>
+__device__ __forceinline__ void collide_fast(const StepArgs<S>& a, const float (&f)[Q],
+                                             long long i, bool dup, bool near_cell) {
+  const long long n = a.n;
+  // opposite pairs (a, b) in the order of js/lbm.js:443-460
+  const float s1 = f[1] + f[2], d1 = f[1] - f[2];
+  const float s3 = f[3] + f[4], d3 = f[3] - f[4];
+  const float s5 = f[5] + f[6], d5 = f[5] - f[6];
+  const float s7 = f[7] + f[8], d7 = f[7] - f[8];
+  const float s9 = f[9] + f[10], d9 = f[9] - f[10];
+  const float s11 = f[11] + f[12], d11 = f[11] - f[12];
+  const float s13 = f[13] + f[14], d13 = f[13] - f[14];
+  const float s15 = f[15] + f[16], d15 = f[15] - f[16];
+  const float s17 = f[17] + f[18], d17 = f[17] - f[18];
+  const float dr = ((f[0] + s1) + (s3 + s5)) + ((s7 + s9) + (s11 + s13)) + (s15 + s17);
+  const float r = 1.0f + dr;
+  if (!(r > 0.0f && r < 3.0e38f)) atomicOr(a.err, 1u);
+  const float inv = __frcp_rn(r);
+  const float vx = ((d1 + d7) + (d9 + d11) + d13) * inv;
+  const float vy = ((d3 + d7) - d9 + (d15 + d17)) * inv;
+  const float vz = ((d5 + d11) - d13 + (d15 - d17)) * inv;
+  if (a.write_fields) {
+    a.rho[i] = r; a.ux[i] = vx; a.uy[i] = vy; a.uz[i] = vz;
+    if (dup) { a.rho[i + 1] = r; a.ux[i + 1] = vx; a.uy[i + 1] = vy; a.uz[i + 1] = vz; }
+  } else if (a.mov && near_cell) {
+    a.rho[i] = r;
+  }
+  const float A = dr - r * 1.5f * (vx * vx + vy * vy + vz * vz);
+  const float r3 = 3.0f * r, r45 = 4.5f * r;
+  constexpr float WF = (float)(1.0 / 18), WE = (float)(1.0 / 36), W0 = (float)(1.0 / 3);
+  // per pair: symmetric equilibrium part es = w(A + 4.5 r cu^2) and
+  // antisymmetric part ea = 3 w r cu; sp = (n_a + n_b)/2, sm = (n_a - n_b)/2
+  const float c1 = vx, c3 = vy, c5 = vz, c7 = vx + vy, c9 = vx - vy, c11 = vx + vz,
+              c13 = vx - vz, c15 = vy + vz, c17 = vy - vz;
+  const float wAF = WF * A, wAE = WE * A, w45F = WF * r45, w45E = WE * r45, w3F = WF * r3,
+              w3E = WE * r3;
+#define WT_PAIR(k, C)                                                          \
+  const float sp##k = fmaf(0.5f, s##k, -fmaf(w45##C * c##k, c##k, wA##C));   \
+  const float sm##k = fmaf(0.5f, d##k, -w3##C * c##k);
+  WT_PAIR(1, F) WT_PAIR(3, F) WT_PAIR(5, F) WT_PAIR(7, E) WT_PAIR(9, E) WT_PAIR(11, E)
+  WT_PAIR(13, E) WT_PAIR(15, E) WT_PAIR(17, E)
+#undef WT_PAIR
+  float om = (float)a.omega0, omm = (float)a.omm0;
+  if (a.les) {
+    // Pi_ab = sum n_q c_qa c_qb from the pair half sums (n_a + n_b = 2 sp)
+    const float sxx = (sp1 + sp7) + (sp9 + sp11) + sp13;
+    const float syy = (sp3 + sp7) + (sp9 + sp15) + sp17;
+    const float szz = (sp5 + sp11) + (sp13 + sp15) + sp17;
+    const float sxy = sp7 - sp9, sxz = sp11 - sp13, syz = sp15 - sp17;
+    const float qq = sxx * sxx + syy * syy + szz * szz + 2.0f * (sxy * sxy + sxz * sxz + syz * syz);
+    // SQ18 * cs2 * |Pi| / r with |Pi| = 2 sqrt(2 qq): 72 cs2 sqrt(qq) / r
+    const float tau0 = (float)a.tau0;
+    const float te = 0.5f * (tau0 + sqrtf(fmaf(tau0, tau0, (float)a.les_c * sqrtf(qq) * inv)));
+    om = __frcp_rn(te);
+    if (a.trt) {
+      const float t5 = te - 0.5f;
+      omm = __fdividef(t5, fmaf(0.5f, t5, (float)a.lam));
+    } else {
+      omm = om;
+    }
+  }
+  S* G = a.G;
+  const float e0 = W0 * A;
+  store_pair(G, i, dup, Store<S>::from_f(fmaf(-om, f[0] - e0, f[0])));
+#define WT_OUT(k, kb)                                                                   \
+  store_pair(G, (long long)(k) * n + i, dup,                                            \
+             Store<S>::from_f(fmaf(-omm, sm##k, fmaf(-om, sp##k, f[k]))));              \
+  store_pair(G, (long long)(kb) * n + i, dup,                                           \
+             Store<S>::from_f(fmaf(omm, sm##k, fmaf(-om, sp##k, f[kb]))));
+  WT_OUT(1, 2) WT_OUT(3, 4) WT_OUT(5, 6) WT_OUT(7, 8) WT_OUT(9, 10) WT_OUT(11, 12) WT_OUT(13, 14)
+  WT_OUT(15, 16) WT_OUT(17, 18)
+#undef WT_OUT
+}
+
+// Float64 collision in the exact operation order of js/lbm.js:377-460. The
+// translation unit that instantiates it is compiled with --fmad=false, so no
+// multiply-add is contracted and every rounding matches the reference's
+// IEEE double arithmetic; results are rounded to S only at the stores.
+template <class S>
+__device__ __forceinline__ void collide_exact(const StepArgs<S>& a, const double (&fq)[Q],
+                                              long long i, bool dup, bool near_cell) {
+  const long long nn = a.n;
+  const double f0 = fq[0], f1 = fq[1], f2 = fq[2], f3 = fq[3], f4 = fq[4], f5 = fq[5],
+               f6 = fq[6], f7 = fq[7], f8 = fq[8], f9 = fq[9], f10 = fq[10], f11 = fq[11],
+               f12 = fq[12], f13 = fq[13], f14 = fq[14], f15 = fq[15], f16 = fq[16],
+               f17 = fq[17], f18 = fq[18];
+  const double dr = f0 + f1 + f2 + f3 + f4 + f5 + f6 + f7 + f8 + f9 + f10 + f11 + f12 + f13 +
+                    f14 + f15 + f16 + f17 + f18;
+  const double r = 1 + dr;
+  if (!(r > 0.0 && r < 1.0e300)) atomicOr(a.err, 1u);
+  const double inv = 1 / r;
+  const double vx = (f1 - f2 + f7 - f8 + f9 - f10 + f11 - f12 + f13 - f14) * inv;
+  const double vy = (f3 - f4 + f7 - f8 - f9 + f10 + f15 - f16 + f17 - f18) * inv;
+  const double vz = (f5 - f6 + f11 - f12 - f13 + f14 + f15 - f16 - f17 + f18) * inv;
+  if (a.write_fields) {
+    const float rf = __double2float_rn(r), xf = __double2float_rn(vx),
+                yf = __double2float_rn(vy), zf = __double2float_rn(vz);
+    a.rho[i] = rf; a.ux[i] = xf; a.uy[i] = yf; a.uz[i] = zf;
+    if (dup) { a.rho[i + 1] = rf; a.ux[i + 1] = xf; a.uy[i + 1] = yf; a.uz[i + 1] = zf; }
+  } else if (a.mov && near_cell) {
+    a.rho[i] = __double2float_rn(r);
+  }
+  const double A = dr - r * 1.5 * (vx * vx + vy * vy + vz * vz);
+  const double r3 = 3 * r, r45 = 4.5 * r;
+  const double ax = vx, ay = vy, az = vz;
+  const double bxy = vx + vy, bxY = vx - vy;
+  const double bxz = vx + vz, bxZ = vx - vz;
+  const double byz = vy + vz, byZ = vy - vz;
+  constexpr double W0 = 1.0 / 3, WF = 1.0 / 18, WE = 1.0 / 36;
+  const double e0 = W0 * A;
+  const double hx = r45 * ax * ax, hy = r45 * ay * ay, hz = r45 * az * az;
+  const double e1 = WF * (A + r3 * ax + hx), e2 = WF * (A - r3 * ax + hx);
+  const double e3 = WF * (A + r3 * ay + hy), e4 = WF * (A - r3 * ay + hy);
+  const double e5 = WF * (A + r3 * az + hz), e6 = WF * (A - r3 * az + hz);
+  const double h7 = r45 * bxy * bxy, h9 = r45 * bxY * bxY;
+  const double h11 = r45 * bxz * bxz, h13 = r45 * bxZ * bxZ;
+  const double h15 = r45 * byz * byz, h17 = r45 * byZ * byZ;
+  const double e7 = WE * (A + r3 * bxy + h7), e8 = WE * (A - r3 * bxy + h7);
+  const double e9 = WE * (A + r3 * bxY + h9), e10 = WE * (A - r3 * bxY + h9);
+  const double e11 = WE * (A + r3 * bxz + h11), e12 = WE * (A - r3 * bxz + h11);
+  const double e13 = WE * (A + r3 * bxZ + h13), e14 = WE * (A - r3 * bxZ + h13);
+  const double e15 = WE * (A + r3 * byz + h15), e16 = WE * (A - r3 * byz + h15);
+  const double e17 = WE * (A + r3 * byZ + h17), e18 = WE * (A - r3 * byZ + h17);
+  const double n1 = f1 - e1, n2 = f2 - e2, n3 = f3 - e3, n4 = f4 - e4;
+  const double n5 = f5 - e5, n6 = f6 - e6, n7 = f7 - e7, n8 = f8 - e8;
+  const double n9 = f9 - e9, n10 = f10 - e10, n11 = f11 - e11, n12 = f12 - e12;
+  const double n13 = f13 - e13, n14 = f14 - e14, n15 = f15 - e15, n16 = f16 - e16;
+  const double n17 = f17 - e17, n18 = f18 - e18;
+  const double tau0 = a.tau0;
+  double om = a.omega0, tauEff = tau0;
+  if (a.les) {
+    const double pxx = n1 + n2 + n7 + n8 + n9 + n10 + n11 + n12 + n13 + n14;
+    const double pyy = n3 + n4 + n7 + n8 + n9 + n10 + n15 + n16 + n17 + n18;
+    const double pzz = n5 + n6 + n11 + n12 + n13 + n14 + n15 + n16 + n17 + n18;
+    const double pxy = n7 + n8 - n9 - n10;
+    const double pxz = n11 + n12 - n13 - n14;
+    const double pyz = n15 + n16 - n17 - n18;
+    const double mag = sqrt(2 * (pxx * pxx + pyy * pyy + pzz * pzz +
+                                 2 * (pxy * pxy + pxz * pxz + pyz * pyz)));
+    const double SQ18 = 18 * 1.4142135623730951;
+    tauEff = 0.5 * (tau0 + sqrt(tau0 * tau0 + SQ18 * a.cs2 * mag * inv));
+    om = 1 / tauEff;
+  }
+  const double omm = a.trt ? 1 / (0.5 + a.lam / (tauEff - 0.5)) : om;
+  S* G = a.G;
+  store_pair(G, 0 * nn + i, dup, Store<S>::from_d(f0 - om * (f0 - e0)));
+  double sp, sm;
+#define WT_XOUT(A_, B_, NA, NB, FA, FB)                                         \
+  sp = 0.5 * (NA + NB); sm = 0.5 * (NA - NB);                                   \
+  store_pair(G, (long long)(A_) * nn + i, dup, Store<S>::from_d(FA - om * sp - omm * sm)); \
+  store_pair(G, (long long)(B_) * nn + i, dup, Store<S>::from_d(FB - om * sp + omm * sm));
+  WT_XOUT(1, 2, n1, n2, f1, f2)
+  WT_XOUT(3, 4, n3, n4, f3, f4)
+  WT_XOUT(5, 6, n5, n6, f5, f6)
+  WT_XOUT(7, 8, n7, n8, f7, f8)
+  WT_XOUT(9, 10, n9, n10, f9, f10)
+  WT_XOUT(11, 12, n11, n12, f11, f12)
+  WT_XOUT(13, 14, n13, n14, f13, f14)
+  WT_XOUT(15, 16, n15, n16, f15, f16)
+  WT_XOUT(17, 18, n17, n18, f17, f18)
+#undef WT_XOUT
+}
+
+template <class S, bool EXACT>
+__global__ void __launch_bounds__(STEP_BX) k_step(const StepArgs<S> a) {
+  using M = typename std::conditional<EXACT, double, float>::type;
+  const int x = blockIdx.x * STEP_BX + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z;
+  const long long i = (long long)x + (long long)a.nx * y + a.nxy * z;
+  int cat = CAT_NONE;
+  bool dup = false;
+  uint8_t fl = 0;
+  if (x < a.nx - 1) {
+    if (x == 0) {
+      cat = CAT_EQ;
+    } else {
+      dup = (x == a.nx - 2);
+      fl = a.flags[i];
+      if (z == 0 || z == a.nz - 1 || y == a.ny - 1) cat = CAT_EQ;
+      else if (fl & FLAG_SOLID_MASK) cat = CAT_KEEP;
+      else if (y == 0) cat = CAT_EQ;
+      else cat = CAT_FLUID;
+    }
+  }
+  double Fx = 0, Fy = 0, Fz = 0;
+  bool link = false;
+  const long long n = a.n;
+  if (cat == CAT_FLUID) {
+    M f[Q];
+    const bool near_cell = (fl & FLAG_NEAR) != 0;
+    const bool shell = a.freeslip && (y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2);
+    if (near_cell || shell) {
+      gather_special<S, M>(a, i, x, y, z, shell, f, Fx, Fy, Fz, link);
+    } else {
+#pragma unroll
+      for (int q = 0; q < Q; q++) {
+        const long long off = ex(q) + (long long)ey(q) * a.nx + (long long)ez(q) * a.nxy;
+        f[q] = ld<M>(a.F[q * n + i - off]);
+      }
+    }
+    if constexpr (EXACT) {
+      collide_exact<S>(a, f, i, dup, near_cell);
+    } else {
+      collide_fast<S>(a, f, i, dup, near_cell);
+    }
+  } else if (cat == CAT_EQ) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) store_pair(a.G, q * n + i, dup, a.eq[q]);
+    if (a.write_fields) {
+      a.ux[i] = a.u0f; a.uy[i] = 0.0f; a.uz[i] = 0.0f; a.rho[i] = 1.0f;
+      if (dup) { a.ux[i + 1] = a.u0f; a.uy[i + 1] = 0.0f; a.uz[i + 1] = 0.0f; a.rho[i + 1] = 1.0f; }
+    }
+  } else if (cat == CAT_KEEP && dup) {
+    // outlet copy of a solid cell in column nx-2: its g is not written this step
+#pragma unroll
+    for (int q = 0; q < Q; q++) a.G[q * n + i + 1] = a.G[q * n + i];
+    if (a.write_fields) {
+      a.ux[i + 1] = a.ux[i]; a.uy[i + 1] = a.uy[i]; a.uz[i + 1] = a.uz[i]; a.rho[i + 1] = a.rho[i];
+    }
+  }
+  block_force_partial(Fx, Fy, Fz, link, a.part);
+}
+
+}  // namespace wt
