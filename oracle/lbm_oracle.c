@@ -42,7 +42,7 @@ static const double OR_W[OR_Q] = {
     1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36,
     1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36};
 /* Mirror images of each direction in y and in z (free-slip option). */
-static const int OR_MY[OR_Q] = {0, 1, 2, 4, 3, 5, 6, 10, 9, 8, 7, 11, 12, 13, 14, 18, 17, 16, 15};
+static const int OR_MY[OR_Q] = {0, 1, 2, 4, 3, 5, 6, 9, 10, 7, 8, 11, 12, 13, 14, 18, 17, 16, 15};
 static const int OR_MZ[OR_Q] = {0, 1, 2, 3, 4, 6, 5, 7, 8, 9, 10, 13, 14, 11, 12, 17, 18, 15, 16};
 
 /* ECMAScript ToInt32 (the `| 0` of js/shapes.js:379 and js/lbm.js:521). */

@@ -127,14 +127,26 @@ def test_fast_f32_within_tolerance(both, side_bc):
 
 
 def test_fast_cfg0_drag_and_fields(both):
-    """Config 0 (128x64x64 sphere, Re=200, TRT 3/16, Cs=0.1, 2000 steps), fast FP32 vs oracle."""
+    """Config 0 (128x64x64 sphere, Re=200, TRT 3/16, Cs=0.1), fast FP32 vs the oracle.
+
+    Pointwise after 200 steps (measured: 1.0e-6 relative on ux). The sphere
+    wake turns unsteady, so pointwise trajectories of different roundings
+    separate after ~700 steps -- the reference's own float32-storage run
+    departs from float64 storage just as fast -- and after 2000 steps the
+    pair-averaged Cd and Cl are compared instead.
+    """
     c = CFG0
     dims = (c["nx"], c["ny"], c["nz"])
     g, o = make_pair(both, dims, "f32", "fast", u0=c["u0"], tau=c["tau"], csm=c["csm"],
                      lam=c["lam"], sphere=c["sphere"], side_bc="freeslip")
-    steps = 2000
-    fg = g.step_forces(steps)
-    fo = o.step_forces(steps, threads=8)
+    fg = [g.step_forces(200)]
+    fo = [o.step_forces(200, threads=8)]
+    gu, ou = g.fields(), o.fields()
+    for name, a, b in zip(("ux", "uy", "uz"), gu[:3], ou[:3]):
+        assert rel_linf(a, b) < 1e-5, name
+    fg.append(g.step_forces(1800))
+    fo.append(o.step_forces(1800, threads=8))
+    fg, fo = np.concatenate(fg), np.concatenate(fo)
     q = 0.5 * c["u0"] ** 2 * g.frontalArea
     cdg = pair_average(fg[:, 0])[-500:].mean() / q
     cdo = pair_average(fo[:, 0])[-500:].mean() / q
@@ -142,9 +154,6 @@ def test_fast_cfg0_drag_and_fields(both):
     clo = pair_average(fo[:, 1])[-500:].mean() / q
     assert abs(cdg - cdo) <= 1e-3 * abs(cdo), (cdg, cdo)
     assert abs(clg - clo) <= 1e-3 * abs(cdo), (clg, clo)
-    gu, ou = g.fields(), o.fields()
-    for name, a, b in zip(("ux", "uy", "uz"), gu[:3], ou[:3]):
-        assert rel_linf(a, b) < 5e-3, name
 
 
 def test_f16dev_within_tolerance(both):
@@ -156,6 +165,22 @@ def test_f16dev_within_tolerance(both):
     cg = pair_average(fg[:, 0])[-100:].mean()
     co = pair_average(fo[:, 0])[-100:].mean()
     assert abs(cg - co) <= 1e-2 * abs(co)
+
+
+@pytest.mark.parametrize("math", ["fast", "exact"])
+@pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
+def test_uniform_flow_is_preserved(both, math, side_bc):
+    """A uniform stream past no body is a fixed point of the step (free-slip exactly)."""
+    LBM, _ = both
+    s = LBM(20, 12, 10, math=math, side_bc=side_bc)
+    s.set_params(u0=0.05, tau=0.512)
+    s.reset()
+    s.step_forces(25)
+    ux, uy, uz, rho = s.fields()
+    tol = 0.0 if (side_bc == "freeslip" and math == "exact") else 1e-6
+    assert np.abs(ux - np.float32(0.05)).max() <= tol * 0.05 + 1e-9
+    assert np.abs(uy).max() <= tol and np.abs(uz).max() <= tol
+    assert np.abs(rho - 1).max() <= tol
 
 
 def test_batch_equals_single_steps(both):
@@ -261,8 +286,9 @@ def test_populations_set_get_round_trip(both):
         data = (rng.standard_normal((19, s.n)) * 1e-3).astype(np.float64)
         s.set_populations(data, "g")
         back = s.populations("g", "f64")
-        tol = {"f32": 1e-10, "f16dev": 1e-6, "f64": 0}[storage]
-        assert np.abs(back - data).max() <= tol
+        # one rounding to the storage type: half an ulp, relative
+        rtol = {"f32": 2.0 ** -24, "f16dev": 2.0 ** -11, "f64": 0.0}[storage]
+        assert np.all(np.abs(back - data) <= rtol * np.abs(data))
 
 
 def test_errors_are_reported(both):

@@ -33,13 +33,25 @@ __host__ __device__ constexpr int opp(int q) {
 }
 // Mirror images in y and in z (free-slip side planes).
 __host__ __device__ constexpr int mirror_y(int q) {
-  constexpr int t[Q] = {0, 1, 2, 4, 3, 5, 6, 10, 9, 8, 7, 11, 12, 13, 14, 18, 17, 16, 15};
+  constexpr int t[Q] = {0, 1, 2, 4, 3, 5, 6, 9, 10, 7, 8, 11, 12, 13, 14, 18, 17, 16, 15};
   return t[q];
 }
 __host__ __device__ constexpr int mirror_z(int q) {
   constexpr int t[Q] = {0, 1, 2, 3, 4, 6, 5, 7, 8, 9, 10, 13, 14, 11, 12, 17, 18, 15, 16};
   return t[q];
 }
+// The opposite and mirror tables must be the index maps they claim to be.
+constexpr bool direction_tables_consistent() {
+  for (int q = 0; q < Q; q++) {
+    if (ex(opp(q)) != -ex(q) || ey(opp(q)) != -ey(q) || ez(opp(q)) != -ez(q)) return false;
+    const int my = mirror_y(q), mz = mirror_z(q);
+    if (ex(my) != ex(q) || ey(my) != -ey(q) || ez(my) != ez(q)) return false;
+    if (ex(mz) != ex(q) || ey(mz) != ey(q) || ez(mz) != -ez(q)) return false;
+  }
+  return true;
+}
+static_assert(direction_tables_consistent(), "D3Q19 opposite / mirror tables are inconsistent");
+
 // Lattice weights (js/lbm.js:34-37), as the IEEE doubles 1/3, 1/18, 1/36.
 __host__ __device__ constexpr double wq(int q) {
   return q == 0 ? 1.0 / 3 : (q <= 6 ? 1.0 / 18 : 1.0 / 36);
