@@ -70,6 +70,14 @@ enum {
                            layer; the plane cells still hold the equilibrium for observers */
 };
 
+/* Which step kernel runs. */
+enum {
+  WT_KERNEL_AUTO = 0,    /* staged when nx allows 16-byte aligned rows, else direct */
+  WT_KERNEL_DIRECT = 1,  /* one thread per cell, populations gathered straight from HBM */
+  WT_KERNEL_STAGED = 2   /* persistent CTAs staging the 19 pull rows with bulk copies (TMA);
+                            needs nx to be a multiple of 16 bytes / element size */
+};
+
 /* Occupancy codes, js/lbm.js:39. */
 enum { WT_FLUID = 0, WT_SOLID_OBJ = 1, WT_SOLID_WALL = 2 };
 
@@ -88,7 +96,7 @@ typedef struct wt_params {
   int32_t moving_walls; /* moving no-slip walls on/off (LBM.movingWalls; set by voxelize) */
   int32_t side_bc;   /* WT_SIDE_EQ (default) or WT_SIDE_FREESLIP */
   int32_t math;      /* WT_MATH_FAST (default) or WT_MATH_EXACT */
-  int32_t reserved;  /* must be 0 */
+  int32_t kernel;    /* WT_KERNEL_AUTO (default), WT_KERNEL_DIRECT or WT_KERNEL_STAGED */
 } wt_params;
 
 /* Body statistics computed by voxelize, js/lbm.js:247-264. */
@@ -103,7 +111,8 @@ typedef struct wt_body_stats {
 
 typedef struct wt_lattice wt_lattice;
 
-/* Reference defaults of js/lbm.js:106-111 (side_bc = WT_SIDE_EQ, math = WT_MATH_FAST). */
+/* Reference defaults of js/lbm.js:106-111 (side_bc = WT_SIDE_EQ, math = WT_MATH_FAST,
+ * kernel = WT_KERNEL_AUTO). */
 void wt_default_params(wt_params* p);
 
 /* new LBM(nx, ny, nz) — js/lbm.js:58-128. Allocates both population buffers,

@@ -28,9 +28,18 @@ def both(wt_lib, oracle_lib):
     return LBM, OracleLBM
 
 
-def make_pair(both, dims, storage="f32", math="exact", **case):
+STAGE_VEC = {"f32": 4, "f16dev": 8, "f64": 2}   # nx must be a multiple for the staged kernel
+
+
+def kernel_or_skip(kernel, nx, storage="f32"):
+    if kernel == "staged" and nx % STAGE_VEC[storage]:
+        pytest.skip(f"staged kernel needs nx % {STAGE_VEC[storage]} == 0")
+    return kernel
+
+
+def make_pair(both, dims, storage="f32", math="exact", kernel="auto", **case):
     LBM, OracleLBM = both
-    g = LBM(*dims, storage=storage, math=math)
+    g = LBM(*dims, storage=storage, math=math, kernel=kernel_or_skip(kernel, dims[0], storage))
     o = OracleLBM(*dims, storage="f64" if storage == "f64" else "f32")
     apply_case(g, **case)
     apply_case(o, **case)
@@ -72,11 +81,18 @@ EXACT_CASES = {
 }
 
 
+EXACT_CASES["staged-shapes"] = dict(dims=(40, 13, 11), sphere=(15.0, 6.5, 5.5, 3.6),
+                                    side_bc="freeslip")
+EXACT_CASES["staged-two-tiles"] = dict(dims=(136, 10, 9), sphere=(126.0, 5.0, 4.5, 3.2),
+                                       ground=True, roadVel=0.03)
+
+
+@pytest.mark.parametrize("kernel", ["direct", "staged"])
 @pytest.mark.parametrize("name", sorted(EXACT_CASES))
-def test_exact_f32_bit_identical(both, name):
+def test_exact_f32_bit_identical(both, name, kernel):
     case = dict(EXACT_CASES[name])
     dims = case.pop("dims")
-    g, o = make_pair(both, dims, "f32", "exact", **case)
+    g, o = make_pair(both, dims, "f32", "exact", kernel=kernel, **case)
     assert_bit_exact(g, o, np.float32)   # after voxelize + seeded init
     for nsteps in (1, 6, 23):
         fg = g.step_forces(nsteps)
@@ -87,31 +103,36 @@ def test_exact_f32_bit_identical(both, name):
     assert g.parity == o.parity
 
 
-@pytest.mark.parametrize("name", ["sphere-default", "freeslip", "ground-rolling-road"])
-def test_exact_f64_bit_identical(both, name):
+@pytest.mark.parametrize("kernel", ["direct", "staged"])
+@pytest.mark.parametrize("name", ["sphere-default", "freeslip", "ground-rolling-road",
+                                  "staged-two-tiles"])
+def test_exact_f64_bit_identical(both, name, kernel):
     case = dict(EXACT_CASES[name])
     dims = case.pop("dims")
-    g, o = make_pair(both, dims, "f64", "exact", **case)
+    g, o = make_pair(both, dims, "f64", "exact", kernel=kernel, **case)
     assert_bit_exact(g, o, np.float64)
     assert_force_close(g.step_forces(17), o.step_forces(17))
     assert_bit_exact(g, o, np.float64)
 
 
-def test_exact_cfg0_shape_bit_identical(both):
+@pytest.mark.parametrize("kernel", ["direct", "staged"])
+def test_exact_cfg0_shape_bit_identical(both, kernel):
     """The 128x64x64 sphere case for 40 steps, oracle on 8 threads (pool decomposition)."""
     c = CFG0
-    g, o = make_pair(both, (c["nx"], c["ny"], c["nz"]), "f32", "exact", u0=c["u0"], tau=c["tau"],
-                     csm=c["csm"], lam=c["lam"], sphere=c["sphere"], side_bc="freeslip")
+    g, o = make_pair(both, (c["nx"], c["ny"], c["nz"]), "f32", "exact", kernel=kernel,
+                     u0=c["u0"], tau=c["tau"], csm=c["csm"], lam=c["lam"], sphere=c["sphere"],
+                     side_bc="freeslip")
     fg = g.step_forces(40)
     fo = o.step_forces(40, threads=8)
     assert_force_close(fg, fo)
     assert_bit_exact(g, o, np.float32)
 
 
+@pytest.mark.parametrize("kernel", ["direct", "staged"])
 @pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
-def test_fast_f32_within_tolerance(both, side_bc):
-    g, o = make_pair(both, (48, 24, 24), "f32", "fast", sphere=(14.0, 12.0, 12.0, 5.0),
-                     side_bc=side_bc)
+def test_fast_f32_within_tolerance(both, side_bc, kernel):
+    g, o = make_pair(both, (48, 24, 24), "f32", "fast", kernel=kernel,
+                     sphere=(14.0, 12.0, 12.0, 5.0), side_bc=side_bc)
     fg = g.step_forces(200)
     fo = o.step_forces(200)
     gu = g.fields()
@@ -156,8 +177,10 @@ def test_fast_cfg0_drag_and_fields(both):
     assert abs(clg - clo) <= 1e-3 * abs(cdo), (clg, clo)
 
 
-def test_f16dev_within_tolerance(both):
-    g, o = make_pair(both, (48, 24, 24), "f16dev", "fast", sphere=(14.0, 12.0, 12.0, 5.0))
+@pytest.mark.parametrize("kernel", ["direct", "staged"])
+def test_f16dev_within_tolerance(both, kernel):
+    g, o = make_pair(both, (48, 24, 24), "f16dev", "fast", kernel=kernel,
+                     sphere=(14.0, 12.0, 12.0, 5.0))
     fg = g.step_forces(200)
     fo = o.step_forces(200)
     gu, ou = g.fields(), o.fields()
@@ -196,6 +219,23 @@ def test_batch_equals_single_steps(both):
         fb.append(b.force)
     assert np.array_equal(fa, np.array(fb))
     assert np.array_equal(a.populations("f", "raw"), b.populations("f", "raw"))
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16dev"])
+def test_staged_matches_direct(both, storage):
+    """Both kernels move the same values; the fast collision may round differently only
+    where the compiler contracts a multiply-add differently, so compare to 1e-6."""
+    LBM, _ = both
+    sims = []
+    for kernel in ("direct", "staged"):
+        s = LBM(64, 20, 18, storage=storage, kernel=kernel, side_bc="freeslip")
+        apply_case(s, sphere=(20.0, 9.0, 9.0, 4.5), side_bc="freeslip", ground=True,
+                   roadVel=0.02)
+        sims.append((s.step_forces(30), s.fields()))
+    (fa, ua), (fb, ub) = sims
+    assert np.abs(fa - fb).max() <= 1e-5 * np.abs(fa).max()
+    for a, b in zip(ua, ub):
+        assert np.abs(a - b).max() <= 1e-6
 
 
 def test_step_is_deterministic(both):

@@ -33,6 +33,10 @@ WT_MATH_EXACT = 1
 WT_SIDE_EQ = 0
 WT_SIDE_FREESLIP = 1
 
+WT_KERNEL_AUTO = 0
+WT_KERNEL_DIRECT = 1
+WT_KERNEL_STAGED = 2
+
 WT_FLUID = 0
 WT_SOLID_OBJ = 1
 WT_SOLID_WALL = 2
@@ -62,7 +66,7 @@ class wt_params(C.Structure):
         ("moving_walls", C.c_int32),
         ("side_bc", C.c_int32),
         ("math", C.c_int32),
-        ("reserved", C.c_int32),
+        ("kernel", C.c_int32),
     ]
 
 

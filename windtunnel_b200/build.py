@@ -34,7 +34,6 @@ UNITS = {
     "wt_kernels_exact.cu": ["--fmad=false"],
     "wt_api.cu": [],
 }
-HEADERS = ["wt_common.cuh", "wt_step.cuh", "wt_internal.h"]
 
 
 def nvcc() -> str:
@@ -55,7 +54,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     """Compile every unit that changed and link libwt.so; returns its path."""
     OBJ_DIR.mkdir(exist_ok=True)
     nv = nvcc()
-    headers = [CSRC / h for h in HEADERS] + [INCLUDE / "wt.h"]
+    headers = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [INCLUDE / "wt.h"]
     objs = []
     for unit, extra in UNITS.items():
         src = CSRC / unit

@@ -68,8 +68,8 @@ long long range_cells(const int rg[6]) {
 
 void free_all(wt_lattice* h) {
   void* dev[] = {h->buf[0], h->buf[1], h->flags, h->ux, h->uy, h->uz, h->rho, h->uwx, h->uwy,
-                 h->uwz, h->part, h->forces_dev, h->err_dev, h->col, h->plan, h->low,
-                 h->counters};
+                 h->uwz, h->part, h->wslot, h->forces_dev, h->err_dev, h->diag_dev, h->col,
+                 h->plan, h->low, h->counters};
   for (void* p : dev)
     if (p) cudaFree(p);
   if (h->forces_host) cudaFreeHost(h->forces_host);
@@ -83,7 +83,9 @@ int check_params(const wt_params* p) {
   if (p->trt && !(p->lambda > 0)) return WT_ERR_ARG;
   if (p->side_bc != WT_SIDE_EQ && p->side_bc != WT_SIDE_FREESLIP) return WT_ERR_ARG;
   if (p->math != WT_MATH_FAST && p->math != WT_MATH_EXACT) return WT_ERR_ARG;
-  if (p->reserved != 0) return WT_ERR_ARG;
+  if (p->kernel != WT_KERNEL_AUTO && p->kernel != WT_KERNEL_DIRECT &&
+      p->kernel != WT_KERNEL_STAGED)
+    return WT_ERR_ARG;
   return WT_OK;
 }
 
@@ -118,48 +120,103 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
   a.flags = h->flags;
   a.ux = h->ux; a.uy = h->uy; a.uz = h->uz; a.rho = h->rho;
   a.uwx = h->uwx; a.uwy = h->uwy; a.uwz = h->uwz;
+  a.wslot = h->wslot;
   a.err = h->err_dev;
+  a.diag = h->diag_dev;
   a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
   a.n = h->n;
   a.nxy = (long long)h->nx * h->ny;
+  for (int q = 0; q < 19; q++) {
+    const long long off = wt::ex(q) + (long long)h->nx * wt::ey(q) + a.nxy * wt::ez(q);
+    a.src[q] = q * h->n - off;
+    a.dst[q] = q * h->n;
+  }
   const wt_params& p = h->p;
   a.tau0 = p.tau;
   a.omega0 = 1 / p.tau;
-  a.omm0 = p.trt ? 1 / (0.5 + p.lambda / (p.tau - 0.5)) : a.omega0;
   a.cs2 = p.csm * p.csm;
   a.lam = p.lambda;
-  a.les_c = 72 * a.cs2;
+  a.tau0f = (float)p.tau;
+  a.omega0f = (float)(1 / p.tau);
+  a.omm0f = (float)(p.trt ? 1 / (0.5 + p.lambda / (p.tau - 0.5)) : 1 / p.tau);
+  a.les_cf = (float)(72 * a.cs2);   // 18*sqrt(2)*cs2*|Pi| with |Pi| = 2*sqrt(2*qq)
+  a.lamf = (float)p.lambda;
+  a.u0f = (float)p.u0;
   a.les = p.les ? 1 : 0;
   a.trt = p.trt ? 1 : 0;
   a.mov = p.moving_walls ? 1 : 0;
   a.freeslip = p.side_bc == WT_SIDE_FREESLIP ? 1 : 0;
+  a.gx = (h->nx + wt::STEP_BX - 1) / wt::STEP_BX;
+  a.units = (long long)a.gx * h->ny * h->nz;
   double eq[19];
   wt::eq_u0_table(p.u0, eq);
   for (int q = 0; q < 19; q++) a.eq[q] = to_store<S>(eq[q]);
-  a.u0f = (float)p.u0;
   return a;
 }
 
-template <class S, class L>
-void run_steps(wt_lattice* h, int nsteps, L launch) {
+// True when the staged (bulk-copy) kernel can run: every row of every
+// direction block starts on a 16-byte boundary.
+bool staged_ok(const wt_lattice* h) { return h->nx % (int)(16 / h->elem) == 0; }
+
+template <class S, class L, class LS>
+void run_steps(wt_lattice* h, int nsteps, bool staged, L launch, LS launch_staged) {
   wt::StepArgs<S> a = make_args<S>(h);
   const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
+  const bool wide = 19 * h->n >= (1LL << 31);
+  const size_t stride = 3 * (size_t)h->nslots;
   for (int done = 0; done < nsteps;) {
     const int chunk = std::min(kChunk, nsteps - done);
     for (int s = 0; s < chunk; s++) {
       a.F = (const S*)h->buf[h->parity];
       a.G = (S*)h->buf[h->parity ^ 1];
-      a.part = h->part + (size_t)s * h->nblocks * 3;
+      a.part = h->part + (size_t)s * stride;
       a.write_fields = (done + s == nsteps - 1) ? 1 : 0;
-      launch(a, grid, h->stream);
+      if (staged) launch_staged(a, h->stream);
+      else launch(a, grid, wide, h->stream);
       h->launches++;
       h->parity ^= 1;
     }
-    wt::launch_force_reduce(h->part, h->nblocks, chunk, h->forces_dev + 3 * (size_t)done,
+    wt::launch_force_reduce(h->part, (unsigned)h->nslots, chunk, h->forces_dev + 3 * (size_t)done,
                             h->stream);
     h->launches++;
     done += chunk;
   }
+}
+
+// Assign a force-partial slot to every step-grid warp that holds a near-wall
+// cell (js/lbm.js:334-359 only accumulates there) and size the partial buffer.
+int rebuild_slots(wt_lattice* h) {
+  uint8_t* mark = nullptr;
+  if (cudaMalloc(&mark, (size_t)h->nwarps) != cudaSuccess)
+    return fail(h, WT_ERR_OOM, "cannot allocate the warp marks");
+  std::vector<uint8_t> hm((size_t)h->nwarps);
+  cudaError_t e = cudaMemsetAsync(mark, 0, (size_t)h->nwarps, h->stream);
+  if (e == cudaSuccess) {
+    wt::launch_mark_warps(h->flags, h->nx, h->ny, h->nz, mark, h->stream);
+    h->launches++;
+    e = cudaMemcpyAsync(hm.data(), mark, hm.size(), cudaMemcpyDeviceToHost, h->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(mark);
+  if (e != cudaSuccess) return cuda_fail(h, e, "rebuild_slots");
+  std::vector<int> slot(hm.size());
+  int n = 0;
+  for (size_t w = 0; w < hm.size(); w++) slot[w] = hm[w] ? n++ : -1;
+  if (n > h->part_cap || !h->part) {
+    if (h->part) cudaFree(h->part);
+    h->part = nullptr;
+    h->part_cap = 0;
+    const int cap = std::max(n, 1);
+    if (cudaMalloc(&h->part, sizeof(double) * 3 * (size_t)cap * kChunk) != cudaSuccess)
+      return fail(h, WT_ERR_OOM, "cannot allocate the force partials");
+    h->part_cap = cap;
+  }
+  e = cudaMemcpyAsync(h->wslot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice,
+                      h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "rebuild_slots upload");
+  h->nslots = n;
+  return WT_OK;
 }
 
 }  // namespace
@@ -212,8 +269,7 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
   h->stats.frontal_area = 1;
   cudaGetDevice(&h->device);
   const dim3 grid = wt::step_grid(nx, ny, nz);
-  h->nblocks = grid.x * grid.y * grid.z;
-  h->part_steps = kChunk;
+  h->nwarps = (long long)grid.x * grid.y * grid.z * wt::STEP_WARPS;
   const size_t pop = (size_t)n * 19 * h->elem;
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaMalloc(&h->buf[0], pop) == cudaSuccess;
@@ -221,9 +277,9 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
   ok = ok && cudaMalloc((void**)&h->flags, (size_t)n) == cudaSuccess;
   float** fl[] = {&h->ux, &h->uy, &h->uz, &h->rho, &h->uwx, &h->uwy, &h->uwz};
   for (float** p : fl) ok = ok && cudaMalloc((void**)p, sizeof(float) * (size_t)n) == cudaSuccess;
-  ok = ok && cudaMalloc((void**)&h->part, sizeof(double) * 3 * (size_t)h->nblocks * kChunk) ==
-                 cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->wslot, sizeof(int) * (size_t)h->nwarps) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->err_dev, sizeof(unsigned)) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->diag_dev, 4 * sizeof(long long)) == cudaSuccess;
   ok = ok && cudaMallocHost((void**)&h->err_host, sizeof(unsigned)) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->col, (size_t)ny * nz) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->plan, (size_t)nx * nz) == cudaSuccess;
@@ -243,6 +299,7 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
   wt::launch_init(h, 0, 0, 0);
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess && rebuild_slots(h) != WT_OK) e = cudaErrorMemoryAllocation;
   if (e != cudaSuccess) {
     g_create_error = std::string("initialisation failed: ") + cudaGetErrorString(e);
     free_all(h);
@@ -276,7 +333,7 @@ int wt_set_params(wt_lattice* h, const wt_params* p) {
   const int c = check_params(p);
   if (c != WT_OK)
     return fail(h, c, "invalid parameters (need finite u0/csm/lambda, tau > 0.5, lambda > 0 "
-                      "with trt, known side_bc and math, reserved = 0)");
+                      "with trt, known side_bc, math and kernel)");
   if (h->storage == WT_STORE_F16DEV && p->math == WT_MATH_EXACT)
     return fail(h, WT_ERR_UNSUPPORTED, "half storage runs the float32 collision only");
   h->p = *p;
@@ -351,7 +408,7 @@ int voxelize_finish(wt_lattice* h, int ground, double road_vel) {
   h->stats.ground = ground ? 1 : 0;
   h->p.moving_walls = (road_vel != 0 || counters[1]) ? 1 : 0;
   h->stats.moving_walls = h->p.moving_walls;
-  return WT_OK;
+  return rebuild_slots(h);
 }
 
 int voxelize_start(wt_lattice* h, int ground, double road_vel) {
@@ -453,17 +510,22 @@ int wt_step(wt_lattice* h, int nsteps, double* forces) {
   int c = grow_forces(h, nsteps);
   if (c != WT_OK) return c;
   WT_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(unsigned), h->stream));
+  WT_CUDA(h, cudaMemsetAsync(h->diag_dev, 0, 4 * sizeof(long long), h->stream));
   const bool exact = h->p.math == WT_MATH_EXACT;
+  bool staged = staged_ok(h) && h->p.kernel != WT_KERNEL_DIRECT;
+  if (h->p.kernel == WT_KERNEL_STAGED && !staged_ok(h))
+    return fail(h, WT_ERR_UNSUPPORTED, "the staged kernel needs nx to be a multiple of " +
+                                           std::to_string(16 / h->elem));
   switch (h->storage) {
     case WT_STORE_F32:
-      if (exact) run_steps<float>(h, nsteps, wt::launch_step_f32_exact);
-      else run_steps<float>(h, nsteps, wt::launch_step_f32_fast);
+      if (exact) run_steps<float>(h, nsteps, staged, wt::launch_step_f32_exact, wt::launch_staged_f32_exact);
+      else run_steps<float>(h, nsteps, staged, wt::launch_step_f32_fast, wt::launch_staged_f32_fast);
       break;
     case WT_STORE_F16DEV:
-      run_steps<__half>(h, nsteps, wt::launch_step_f16_fast);
+      run_steps<__half>(h, nsteps, staged, wt::launch_step_f16_fast, wt::launch_staged_f16_fast);
       break;
     default:
-      run_steps<double>(h, nsteps, wt::launch_step_f64_exact);
+      run_steps<double>(h, nsteps, staged, wt::launch_step_f64_exact, wt::launch_staged_f64_exact);
       break;
   }
   WT_CUDA(h, cudaGetLastError());
@@ -476,7 +538,21 @@ int wt_step(wt_lattice* h, int nsteps, double* forces) {
   const double* last = h->forces_host + 3 * (size_t)(nsteps - 1);
   h->force[0] = last[0]; h->force[1] = last[1]; h->force[2] = last[2];
   if (forces) memcpy(forces, h->forces_host, sizeof(double) * 3 * (size_t)nsteps);
-  if (*h->err_host)
+  if (*h->err_host & 4u)
+    return fail(h, WT_ERR_TIMEOUT, "a staged row copy did not complete within its wait budget");
+  if (*h->err_host & 8u) {
+    long long d[4] = {0, 0, 0, 0};
+    cudaMemcpy(d, h->diag_dev, sizeof(d), cudaMemcpyDeviceToHost);
+    return fail(h, WT_ERR_STATE,
+                std::string("a staged row ") + (d[0] == 2 ? "store" : "load") +
+                    " would have been misaligned or left its buffer and was skipped (direction " +
+                    std::to_string(d[1]) + ", unit " + std::to_string(d[2]) + ", element offset " +
+                    std::to_string(d[3]) + ")");
+  }
+  if (*h->err_host & 2u)
+    return fail(h, WT_ERR_STATE, "a near-wall warp had no force slot (occupancy changed "
+                                 "without voxelize)");
+  if (*h->err_host & 1u)
     return fail(h, WT_ERR_DIVERGED, "a step produced a non-finite or non-positive density");
   return WT_OK;
 }
@@ -654,7 +730,7 @@ int wt_set_state(wt_lattice* h, const void* in, size_t bytes) {
   memcpy(h->force, hd.force, sizeof(hd.force));
   h->p = hd.params;
   h->stats = hd.stats;
-  return WT_OK;
+  return rebuild_slots(h);
 }
 
 int wt_sample(wt_lattice* h, const double* xyz, int npts, double* out) {

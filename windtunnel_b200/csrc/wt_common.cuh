@@ -110,23 +110,37 @@ struct StepArgs {
   const float* uwx;
   const float* uwy;
   const float* uwz;
-  double* part;        // this step's per-block force partials, 3 per block
+  double* part;        // this step's force partials, 3 per warp slot
+  const int* wslot;    // per warp of the grid: its partial slot, or -1 (no wall cell)
   unsigned* err;       // bit 0: non-finite / non-positive density seen
+  long long* diag;     // first rejected staged copy: {kind, q, unit, element offset}
   int nx, ny, nz;
   long long n;         // nx*ny*nz
   long long nxy;       // nx*ny
-  double tau0, omega0, omm0, cs2, lam;
-  double les_c;        // 72*cs2: the LES constant folded for the fast body
+  long long src[Q];    // pull offset of direction q: q*n - (ex + nx*ey + nxy*ez)
+  long long dst[Q];    // store offset of direction q: q*n
+  // float64 parameters (exact collision)
+  double tau0, omega0, cs2, lam;
+  // float32 parameters (fast collision), rounded once on the host
+  float tau0f, omega0f, omm0f, les_cf, lamf, u0f;
   int les, trt, mov, freeslip, write_fields;
+  int gx;              // x-segments (units) per row
+  long long units;     // gx*ny*nz
   S eq[Q];             // equilibrium deviation at rho=1, u=(u0,0,0), rounded to S
-  float u0f;           // (float)u0 for the boundary-cell fields
 };
 
 // Block shape of the fused step: one thread per cell along x.
 constexpr int STEP_BX = 128;
+constexpr int STEP_WARPS = STEP_BX / 32;
 
 inline dim3 step_grid(int nx, int ny, int nz) {
   return dim3((unsigned)((nx + STEP_BX - 1) / STEP_BX), (unsigned)ny, (unsigned)nz);
+}
+
+// Warp of the step grid that holds cell (x, y, z).
+__host__ __device__ inline long long step_warp_of(int x, int y, int z, int nx, int ny) {
+  const int gx = (nx + STEP_BX - 1) / STEP_BX;
+  return (((long long)z * ny + y) * gx + x / STEP_BX) * STEP_WARPS + (x % STEP_BX) / 32;
 }
 
 }  // namespace wt

@@ -27,15 +27,18 @@ struct wt_lattice {
   float* uwx = nullptr;          // wall velocities of solid cells (js/lbm.js:92-94)
   float* uwy = nullptr;
   float* uwz = nullptr;
-  // per-step force reduction
-  unsigned nblocks = 0;          // blocks of one step launch
-  int part_steps = 0;            // steps whose partials fit in `part`
+  // per-step force reduction: one partial per warp that holds a near-wall cell
+  long long nwarps = 0;          // warps of one step launch
+  int* wslot = nullptr;          // per warp: partial slot or -1
+  int nslots = 0;                // warps with a slot
+  int part_cap = 0;              // slots that fit in `part` (per step of a chunk)
   double* part = nullptr;
   double* forces_dev = nullptr;
   double* forces_host = nullptr; // pinned
   int forces_cap = 0;            // steps that fit in forces_dev / forces_host
   unsigned* err_dev = nullptr;
   unsigned* err_host = nullptr;  // pinned
+  long long* diag_dev = nullptr; // first rejected staged copy {kind, q, unit, offset}
   // voxelize statistics scratch
   uint8_t* col = nullptr;        // ny*nz frontal projection
   uint8_t* plan = nullptr;       // nx*nz planform projection
@@ -53,14 +56,25 @@ struct wt_lattice {
 namespace wt {
 
 // Step launchers (one per storage x arithmetic pair that is provided).
-void launch_step_f32_fast(const StepArgs<float>& a, dim3 grid, cudaStream_t s);
-void launch_step_f16_fast(const StepArgs<__half>& a, dim3 grid, cudaStream_t s);
-void launch_step_f32_exact(const StepArgs<float>& a, dim3 grid, cudaStream_t s);
-void launch_step_f64_exact(const StepArgs<double>& a, dim3 grid, cudaStream_t s);
+// `wide` selects 64-bit direction offsets (19*n beyond 31 bits).
+void launch_step_f32_fast(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_step_f16_fast(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_step_f32_exact(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_step_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cudaStream_t s);
 
-// Deterministic per-step sum of the block partials: out[3*s..3*s+2].
-void launch_force_reduce(const double* part, unsigned nblocks, int nsteps, double* out,
+// Staged (bulk-copy) step launchers; need nx % (16 / sizeof(S)) == 0.
+void launch_staged_f32_fast(const StepArgs<float>& a, cudaStream_t s);
+void launch_staged_f16_fast(const StepArgs<__half>& a, cudaStream_t s);
+void launch_staged_f32_exact(const StepArgs<float>& a, cudaStream_t s);
+void launch_staged_f64_exact(const StepArgs<double>& a, cudaStream_t s);
+
+// Deterministic per-step sum of the warp partials: out[3*s..3*s+2].
+void launch_force_reduce(const double* part, unsigned nslots, int nsteps, double* out,
                          cudaStream_t s);
+
+// mark[w] = 1 for every step-grid warp w holding a near-wall cell.
+void launch_mark_warps(const uint8_t* flags, int nx, int ny, int nz, uint8_t* mark,
+                       cudaStream_t s);
 
 // Equilibrium initialisation of both buffers and the fields:
 // mode 0 = reset(), mode 1 = reset() + seeded noise.

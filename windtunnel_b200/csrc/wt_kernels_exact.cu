@@ -7,16 +7,26 @@
 #include <math.h>
 
 #include "wt_internal.h"
-#include "wt_step.cuh"
+#include "wt_staged_launch.cuh"
 
 namespace wt {
 
-void launch_step_f32_exact(const StepArgs<float>& a, dim3 grid, cudaStream_t s) {
-  k_step<float, true><<<grid, STEP_BX, 0, s>>>(a);
+void launch_step_f32_exact(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s) {
+  if (wide) k_step<float, true, long long><<<grid, STEP_BX, 0, s>>>(a);
+  else k_step<float, true, int><<<grid, STEP_BX, 0, s>>>(a);
 }
 
-void launch_step_f64_exact(const StepArgs<double>& a, dim3 grid, cudaStream_t s) {
-  k_step<double, true><<<grid, STEP_BX, 0, s>>>(a);
+void launch_step_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cudaStream_t s) {
+  if (wide) k_step<double, true, long long><<<grid, STEP_BX, 0, s>>>(a);
+  else k_step<double, true, int><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+void launch_staged_f32_exact(const StepArgs<float>& a, cudaStream_t s) {
+  launch_staged<float, true>(a, s);
+}
+
+void launch_staged_f64_exact(const StepArgs<double>& a, cudaStream_t s) {
+  launch_staged<double, true>(a, s);
 }
 
 // ---- helpers -----------------------------------------------------------------

@@ -2,19 +2,47 @@
 // (float32 and half-deviation storage), plus the force reduction. Built with
 // the default multiply-add contraction.
 #include "wt_internal.h"
-#include "wt_step.cuh"
+#include "wt_staged_launch.cuh"
 
 namespace wt {
 
-void launch_step_f32_fast(const StepArgs<float>& a, dim3 grid, cudaStream_t s) {
-  k_step<float, false><<<grid, STEP_BX, 0, s>>>(a);
+void launch_step_f32_fast(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s) {
+  if (wide) k_step<float, false, long long><<<grid, STEP_BX, 0, s>>>(a);
+  else k_step<float, false, int><<<grid, STEP_BX, 0, s>>>(a);
 }
 
-void launch_step_f16_fast(const StepArgs<__half>& a, dim3 grid, cudaStream_t s) {
-  k_step<__half, false><<<grid, STEP_BX, 0, s>>>(a);
+void launch_step_f16_fast(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s) {
+  if (wide) k_step<__half, false, long long><<<grid, STEP_BX, 0, s>>>(a);
+  else k_step<__half, false, int><<<grid, STEP_BX, 0, s>>>(a);
 }
 
-// One block per step; each thread sums a fixed strided subset of the block
+void launch_staged_f32_fast(const StepArgs<float>& a, cudaStream_t s) {
+  launch_staged<float, false>(a, s);
+}
+
+void launch_staged_f16_fast(const StepArgs<__half>& a, cudaStream_t s) {
+  launch_staged<__half, false>(a, s);
+}
+
+// Marks the warps of the step grid that hold at least one near-wall cell.
+__global__ void k_mark_warps(const uint8_t* __restrict__ flags, int nx, int ny, int nz,
+                             uint8_t* __restrict__ mark) {
+  const long long n = (long long)nx * ny * nz;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (flags[i] & FLAG_NEAR) {
+      const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long long)nx * ny));
+      mark[step_warp_of(x, y, z, nx, ny)] = 1;
+    }
+  }
+}
+
+void launch_mark_warps(const uint8_t* flags, int nx, int ny, int nz, uint8_t* mark,
+                       cudaStream_t s) {
+  k_mark_warps<<<148 * 16, 256, 0, s>>>(flags, nx, ny, nz, mark);
+}
+
+// One block per step; each thread sums a fixed strided subset of the warp
 // partials, then a fixed-shape tree combines them. The order never depends
 // on timing, so the force series is reproducible run to run.
 constexpr int RED_T = 256;
@@ -49,9 +77,9 @@ __global__ void __launch_bounds__(RED_T) k_force_reduce(const double* __restrict
   }
 }
 
-void launch_force_reduce(const double* part, unsigned nblocks, int nsteps, double* out,
+void launch_force_reduce(const double* part, unsigned nslots, int nsteps, double* out,
                          cudaStream_t s) {
-  k_force_reduce<<<nsteps, RED_T, 0, s>>>(part, nblocks, out);
+  k_force_reduce<<<nsteps, RED_T, 0, s>>>(part, nslots, out);
 }
 
 }  // namespace wt

@@ -29,37 +29,116 @@ __device__ __forceinline__ M ld(S v) {
   else return Store<S>::load_f(v);
 }
 
+// Output writers of the collision: into a register array (direct kernel) or
+// straight into a shared-memory output tile (staged kernel).
+template <class S>
+struct RegOut {
+  S (&o)[Q];
+  __device__ __forceinline__ void put(int q, S v) { o[q] = v; }
+};
+template <class S>
+struct TileOut {
+  S* base;      // &tile[0][t]; direction q lives at base[q * stride]
+  int stride;
+  __device__ __forceinline__ void put(int q, S v) { base[q * stride] = v; }
+};
+
 enum : int { CAT_NONE = 0, CAT_EQ = 1, CAT_KEEP = 2, CAT_FLUID = 3 };
 
-// Sum three doubles over the block in a fixed order and store them at
-// part[3*block]. Every thread of the block must call it.
-__device__ __forceinline__ void block_force_partial(double fx, double fy, double fz, bool link,
-                                                    double* part) {
-  __shared__ double red[3][STEP_BX / 32];
-  const unsigned blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-  if (__syncthreads_or(link)) {
+// Sum three doubles over the warp in a fixed order and store them in the
+// warp's partial slot. Exactly the warps that hold a near-wall cell own a slot
+// (the table is rebuilt by voxelize), and each of them writes its slot every
+// step -- zeros when none of its links touches the body -- so the ~all-fluid
+// warps write nothing and no block-wide barrier is needed. Every lane of the
+// warp must call it; `near_cell` marks a computed near-wall cell.
+template <class S>
+__device__ __forceinline__ void warp_force_partial_w(double fx, double fy, double fz,
+                                                     bool near_cell, const StepArgs<S>& a,
+                                                     long long warp_id) {
+  if (__any_sync(0xffffffffu, near_cell)) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       fx += __shfl_down_sync(0xffffffffu, fx, o);
       fy += __shfl_down_sync(0xffffffffu, fy, o);
       fz += __shfl_down_sync(0xffffffffu, fz, o);
     }
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { red[0][w] = fx; red[1][w] = fy; red[2][w] = fz; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double sx = 0, sy = 0, sz = 0;
-#pragma unroll
-      for (int k = 0; k < STEP_BX / 32; k++) { sx += red[0][k]; sy += red[1][k]; sz += red[2][k]; }
-      part[3 * (size_t)blk] = sx;
-      part[3 * (size_t)blk + 1] = sy;
-      part[3 * (size_t)blk + 2] = sz;
+    if ((threadIdx.x & 31) == 0) {
+      const int slot = a.wslot[warp_id];
+      if (slot >= 0) {
+        a.part[3 * (size_t)slot] = fx;
+        a.part[3 * (size_t)slot + 1] = fy;
+        a.part[3 * (size_t)slot + 2] = fz;
+      } else {
+        atomicOr(a.err, 2u);   // slot table out of date: reported, never silently dropped
+      }
     }
-  } else if (threadIdx.x == 0) {
-    part[3 * (size_t)blk] = 0;
-    part[3 * (size_t)blk + 1] = 0;
-    part[3 * (size_t)blk + 2] = 0;
   }
+}
+
+// Warp partial of the direct kernel, whose block b covers unit b.
+template <class S>
+__device__ __forceinline__ void warp_force_partial(double fx, double fy, double fz,
+                                                   bool near_cell, const StepArgs<S>& a) {
+  const long long b = (long long)(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  warp_force_partial_w(fx, fy, fz, near_cell, a, b * STEP_WARPS + (threadIdx.x >> 5));
+}
+
+// Warp partial of the staged kernel, processing unit u.
+template <class S>
+__device__ __forceinline__ void warp_force_partial_unit(double fx, double fy, double fz,
+                                                        bool near_cell, const StepArgs<S>& a,
+                                                        long long u) {
+  warp_force_partial_w(fx, fy, fz, near_cell, a, u * STEP_WARPS + (threadIdx.x >> 5));
+}
+
+// Bounce-back link q of cell i toward solid neighbour j (code s):
+// js/lbm.js:339-359. Returns the pulled population and accumulates the
+// momentum exchange of links into the body (SOLID_OBJ).
+template <class S, class M, int q>
+__device__ __forceinline__ M bounce_link(const StepArgs<S>& a, long long i, long long j, int s,
+                                         M rho_prev, double& Fx, double& Fy, double& Fz) {
+  const M fd = ld<M>(a.F[opp(q) * a.n + i]);
+  M corr = 0;
+  if (a.mov) {
+    const M cu = (M)ex(q) * (M)a.uwx[j] + (M)ey(q) * (M)a.uwy[j] + (M)ez(q) * (M)a.uwz[j];
+    if (cu != (M)0) corr = (M)6 * (M)wq(q) * rho_prev * cu;
+  }
+  if (s == WT_SOLID_OBJ) {
+    const M d = (M)2 * fd + corr;
+    Fx -= (double)(d * (M)ex(q));
+    Fy -= (double)(d * (M)ey(q));
+    Fz -= (double)(d * (M)ez(q));
+  }
+  return fd + corr;
+}
+
+// Overwrite, in f (already holding the plain pulled values), the directions
+// whose source is solid (bounce-back) or lies on a free-slip side plane
+// (mirror gather). Used by the staged kernel.
+template <class S, class M>
+__device__ __forceinline__ void patch_special(const StepArgs<S>& a, long long i, int x, int y,
+                                              int z, bool shell, M (&f)[Q], double& Fx,
+                                              double& Fy, double& Fz) {
+  const M rho_prev = (M)(a.mov ? a.rho[i] : 1.0f);
+#define WT_PATCH(q)                                                                       \
+  {                                                                                       \
+    const long long j = i - (ex(q) + (long long)ey(q) * a.nx + (long long)ez(q) * a.nxy); \
+    const int s = a.flags[j] & FLAG_SOLID_MASK;                                           \
+    if (s) {                                                                              \
+      f[q] = bounce_link<S, M, q>(a, i, j, s, rho_prev, Fx, Fy, Fz);                      \
+    } else if (shell) {                                                                   \
+      int sy = y - ey(q), sz = z - ez(q), qq = q;                                         \
+      bool refl = false;                                                                  \
+      if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); refl = true; }          \
+      if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); refl = true; }          \
+      if (refl)                                                                           \
+        f[q] = ld<M>(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);    \
+    }                                                                                     \
+  }
+  WT_PATCH(1) WT_PATCH(2) WT_PATCH(3) WT_PATCH(4) WT_PATCH(5) WT_PATCH(6) WT_PATCH(7)
+  WT_PATCH(8) WT_PATCH(9) WT_PATCH(10) WT_PATCH(11) WT_PATCH(12) WT_PATCH(13) WT_PATCH(14)
+  WT_PATCH(15) WT_PATCH(16) WT_PATCH(17) WT_PATCH(18)
+#undef WT_PATCH
 }
 
 // Gather for cells next to a solid (bounce-back + momentum exchange,
@@ -67,7 +146,7 @@ __device__ __forceinline__ void block_force_partial(double fx, double fy, double
 template <class S, class M>
 __device__ __forceinline__ void gather_special(const StepArgs<S>& a, long long i, int x, int y,
                                                int z, bool shell, M (&f)[Q], double& Fx,
-                                               double& Fy, double& Fz, bool& link) {
+                                               double& Fy, double& Fz) {
   const long long n = a.n;
   const M rho_prev = (M)(a.mov ? a.rho[i] : 1.0f);
 #pragma unroll
@@ -88,7 +167,6 @@ __device__ __forceinline__ void gather_special(const StepArgs<S>& a, long long i
         Fx -= (double)(d * (M)ex(q));
         Fy -= (double)(d * (M)ey(q));
         Fz -= (double)(d * (M)ez(q));
-        link = true;
       }
     } else {
       long long src = q * n + i - off;
@@ -103,20 +181,13 @@ __device__ __forceinline__ void gather_special(const StepArgs<S>& a, long long i
   }
 }
 
-template <class S>
-__device__ __forceinline__ void store_pair(S* G, long long idx, bool dup, S v) {
-  G[idx] = v;
-  if (dup) G[idx + 1] = v;
-}
-
 // Float32 collision, re-associated: opposite pairs are carried as half sums
 // and half differences, so moments, the equilibrium, the stress tensor of the
 // Smagorinsky model and the TRT update share their partial results. The
 // mathematics is that of js/lbm.js:377-460; only the rounding differs.
-template <class S>
+template <class S, class Out>
 __device__ __forceinline__ void collide_fast(const StepArgs<S>& a, const float (&f)[Q],
-                                             long long i, bool dup, bool near_cell) {
-  const long long n = a.n;
+                                             long long i, bool dup, bool near_cell, Out out) {
   // opposite pairs (a, b) in the order of js/lbm.js:443-460
   const float s1 = f[1] + f[2], d1 = f[1] - f[2];
   const float s3 = f[3] + f[4], d3 = f[3] - f[4];
@@ -155,7 +226,7 @@ __device__ __forceinline__ void collide_fast(const StepArgs<S>& a, const float (
   WT_PAIR(1, F) WT_PAIR(3, F) WT_PAIR(5, F) WT_PAIR(7, E) WT_PAIR(9, E) WT_PAIR(11, E)
   WT_PAIR(13, E) WT_PAIR(15, E) WT_PAIR(17, E)
 #undef WT_PAIR
-  float om = (float)a.omega0, omm = (float)a.omm0;
+  float om = a.omega0f, omm = a.omm0f;
   if (a.les) {
     // Pi_ab = sum n_q c_qa c_qb from the pair half sums (n_a + n_b = 2 sp)
     const float sxx = (sp1 + sp7) + (sp9 + sp11) + sp13;
@@ -164,24 +235,21 @@ __device__ __forceinline__ void collide_fast(const StepArgs<S>& a, const float (
     const float sxy = sp7 - sp9, sxz = sp11 - sp13, syz = sp15 - sp17;
     const float qq = sxx * sxx + syy * syy + szz * szz + 2.0f * (sxy * sxy + sxz * sxz + syz * syz);
     // SQ18 * cs2 * |Pi| / r with |Pi| = 2 sqrt(2 qq): 72 cs2 sqrt(qq) / r
-    const float tau0 = (float)a.tau0;
-    const float te = 0.5f * (tau0 + sqrtf(fmaf(tau0, tau0, (float)a.les_c * sqrtf(qq) * inv)));
+    const float tau0 = a.tau0f;
+    const float te = 0.5f * (tau0 + sqrtf(fmaf(tau0, tau0, a.les_cf * sqrtf(qq) * inv)));
     om = __frcp_rn(te);
     if (a.trt) {
       const float t5 = te - 0.5f;
-      omm = __fdividef(t5, fmaf(0.5f, t5, (float)a.lam));
+      omm = __fdividef(t5, fmaf(0.5f, t5, a.lamf));
     } else {
       omm = om;
     }
   }
-  S* G = a.G;
   const float e0 = W0 * A;
-  store_pair(G, i, dup, Store<S>::from_f(fmaf(-om, f[0] - e0, f[0])));
-#define WT_OUT(k, kb)                                                                   \
-  store_pair(G, (long long)(k) * n + i, dup,                                            \
-             Store<S>::from_f(fmaf(-omm, sm##k, fmaf(-om, sp##k, f[k]))));              \
-  store_pair(G, (long long)(kb) * n + i, dup,                                           \
-             Store<S>::from_f(fmaf(omm, sm##k, fmaf(-om, sp##k, f[kb]))));
+  out.put(0, Store<S>::from_f(fmaf(-om, f[0] - e0, f[0])));
+#define WT_OUT(k, kb)                                                          \
+  out.put(k, Store<S>::from_f(fmaf(-omm, sm##k, fmaf(-om, sp##k, f[k]))));     \
+  out.put(kb, Store<S>::from_f(fmaf(omm, sm##k, fmaf(-om, sp##k, f[kb]))));
   WT_OUT(1, 2) WT_OUT(3, 4) WT_OUT(5, 6) WT_OUT(7, 8) WT_OUT(9, 10) WT_OUT(11, 12) WT_OUT(13, 14)
   WT_OUT(15, 16) WT_OUT(17, 18)
 #undef WT_OUT
@@ -191,10 +259,9 @@ __device__ __forceinline__ void collide_fast(const StepArgs<S>& a, const float (
 // translation unit that instantiates it is compiled with --fmad=false, so no
 // multiply-add is contracted and every rounding matches the reference's
 // IEEE double arithmetic; results are rounded to S only at the stores.
-template <class S>
+template <class S, class Out>
 __device__ __forceinline__ void collide_exact(const StepArgs<S>& a, const double (&fq)[Q],
-                                              long long i, bool dup, bool near_cell) {
-  const long long nn = a.n;
+                                              long long i, bool dup, bool near_cell, Out out) {
   const double f0 = fq[0], f1 = fq[1], f2 = fq[2], f3 = fq[3], f4 = fq[4], f5 = fq[5],
                f6 = fq[6], f7 = fq[7], f8 = fq[8], f9 = fq[9], f10 = fq[10], f11 = fq[11],
                f12 = fq[12], f13 = fq[13], f14 = fq[14], f15 = fq[15], f16 = fq[16],
@@ -257,13 +324,12 @@ __device__ __forceinline__ void collide_exact(const StepArgs<S>& a, const double
     om = 1 / tauEff;
   }
   const double omm = a.trt ? 1 / (0.5 + a.lam / (tauEff - 0.5)) : om;
-  S* G = a.G;
-  store_pair(G, 0 * nn + i, dup, Store<S>::from_d(f0 - om * (f0 - e0)));
+  out.put(0, Store<S>::from_d(f0 - om * (f0 - e0)));
   double sp, sm;
-#define WT_XOUT(A_, B_, NA, NB, FA, FB)                                         \
-  sp = 0.5 * (NA + NB); sm = 0.5 * (NA - NB);                                   \
-  store_pair(G, (long long)(A_) * nn + i, dup, Store<S>::from_d(FA - om * sp - omm * sm)); \
-  store_pair(G, (long long)(B_) * nn + i, dup, Store<S>::from_d(FB - om * sp + omm * sm));
+#define WT_XOUT(A_, B_, NA, NB, FA, FB)                   \
+  sp = 0.5 * (NA + NB); sm = 0.5 * (NA - NB);             \
+  out.put(A_, Store<S>::from_d(FA - om * sp - omm * sm)); \
+  out.put(B_, Store<S>::from_d(FB - om * sp + omm * sm));
   WT_XOUT(1, 2, n1, n2, f1, f2)
   WT_XOUT(3, 4, n3, n4, f3, f4)
   WT_XOUT(5, 6, n5, n6, f5, f6)
@@ -276,64 +342,80 @@ __device__ __forceinline__ void collide_exact(const StepArgs<S>& a, const double
 #undef WT_XOUT
 }
 
-template <class S, bool EXACT>
-__global__ void __launch_bounds__(STEP_BX) k_step(const StepArgs<S> a) {
+// The float32 step is capped at 64 registers so that 8 blocks of 128 threads
+// stay resident per SM: the step is bound by memory latency, and resident
+// warps are what keep enough of the 19 load streams in flight. The float64
+// (exact) step keeps 128 registers rather than spill.
+constexpr int step_min_blocks(bool exact) { return exact ? 4 : 8; }
+
+// IDX is the type of the per-direction offsets: int when 19*n fits in 31
+// bits (every practical lattice), long long otherwise.
+template <class S, bool EXACT, class IDX>
+__global__ void __launch_bounds__(STEP_BX, step_min_blocks(EXACT)) k_step(const StepArgs<S> a) {
   using M = typename std::conditional<EXACT, double, float>::type;
   const int x = blockIdx.x * STEP_BX + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
   const long long i = (long long)x + (long long)a.nx * y + a.nxy * z;
-  int cat = CAT_NONE;
-  bool dup = false;
-  uint8_t fl = 0;
+  double Fx = 0, Fy = 0, Fz = 0;
+  bool near_cell = false;
   if (x < a.nx - 1) {
+    int cat;
+    uint8_t fl = 0;
+    const bool dup = (x == a.nx - 2);   // this thread also writes the outlet cell x+1
     if (x == 0) {
       cat = CAT_EQ;
     } else {
-      dup = (x == a.nx - 2);
       fl = a.flags[i];
       if (z == 0 || z == a.nz - 1 || y == a.ny - 1) cat = CAT_EQ;
       else if (fl & FLAG_SOLID_MASK) cat = CAT_KEEP;
       else if (y == 0) cat = CAT_EQ;
       else cat = CAT_FLUID;
     }
-  }
-  double Fx = 0, Fy = 0, Fz = 0;
-  bool link = false;
-  const long long n = a.n;
-  if (cat == CAT_FLUID) {
-    M f[Q];
-    const bool near_cell = (fl & FLAG_NEAR) != 0;
-    const bool shell = a.freeslip && (y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2);
-    if (near_cell || shell) {
-      gather_special<S, M>(a, i, x, y, z, shell, f, Fx, Fy, Fz, link);
-    } else {
+    S* Gi = a.G + i;
+    if (cat == CAT_FLUID) {
+      M f[Q];
+      near_cell = (fl & FLAG_NEAR) != 0;
+      const bool shell = a.freeslip && (y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2);
+      if (near_cell || shell) {
+        gather_special<S, M>(a, i, x, y, z, shell, f, Fx, Fy, Fz);
+      } else {
+        const S* Fi = a.F + i;
 #pragma unroll
-      for (int q = 0; q < Q; q++) {
-        const long long off = ex(q) + (long long)ey(q) * a.nx + (long long)ez(q) * a.nxy;
-        f[q] = ld<M>(a.F[q * n + i - off]);
+        for (int q = 0; q < Q; q++) f[q] = ld<M>(Fi[(IDX)a.src[q]]);
+      }
+      S out[Q];
+      if constexpr (EXACT) {
+        collide_exact<S>(a, f, i, dup, near_cell, RegOut<S>{out});
+      } else {
+        collide_fast<S>(a, f, i, dup, near_cell, RegOut<S>{out});
+      }
+#pragma unroll
+      for (int q = 0; q < Q; q++) Gi[(IDX)a.dst[q]] = out[q];
+      if (dup) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) Gi[(IDX)a.dst[q] + 1] = out[q];
+      }
+    } else if (cat == CAT_EQ) {
+#pragma unroll
+      for (int q = 0; q < Q; q++) Gi[(IDX)a.dst[q]] = a.eq[q];
+      if (dup) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) Gi[(IDX)a.dst[q] + 1] = a.eq[q];
+      }
+      if (a.write_fields) {
+        a.ux[i] = a.u0f; a.uy[i] = 0.0f; a.uz[i] = 0.0f; a.rho[i] = 1.0f;
+        if (dup) { a.ux[i + 1] = a.u0f; a.uy[i + 1] = 0.0f; a.uz[i + 1] = 0.0f; a.rho[i + 1] = 1.0f; }
+      }
+    } else if (dup) {
+      // outlet copy of a solid cell in column nx-2: its g is not written this step
+#pragma unroll
+      for (int q = 0; q < Q; q++) Gi[(IDX)a.dst[q] + 1] = Gi[(IDX)a.dst[q]];
+      if (a.write_fields) {
+        a.ux[i + 1] = a.ux[i]; a.uy[i + 1] = a.uy[i]; a.uz[i + 1] = a.uz[i]; a.rho[i + 1] = a.rho[i];
       }
     }
-    if constexpr (EXACT) {
-      collide_exact<S>(a, f, i, dup, near_cell);
-    } else {
-      collide_fast<S>(a, f, i, dup, near_cell);
-    }
-  } else if (cat == CAT_EQ) {
-#pragma unroll
-    for (int q = 0; q < Q; q++) store_pair(a.G, q * n + i, dup, a.eq[q]);
-    if (a.write_fields) {
-      a.ux[i] = a.u0f; a.uy[i] = 0.0f; a.uz[i] = 0.0f; a.rho[i] = 1.0f;
-      if (dup) { a.ux[i + 1] = a.u0f; a.uy[i + 1] = 0.0f; a.uz[i + 1] = 0.0f; a.rho[i + 1] = 1.0f; }
-    }
-  } else if (cat == CAT_KEEP && dup) {
-    // outlet copy of a solid cell in column nx-2: its g is not written this step
-#pragma unroll
-    for (int q = 0; q < Q; q++) a.G[q * n + i + 1] = a.G[q * n + i];
-    if (a.write_fields) {
-      a.ux[i + 1] = a.ux[i]; a.uy[i + 1] = a.uy[i]; a.uz[i + 1] = a.uz[i]; a.rho[i + 1] = a.rho[i];
-    }
   }
-  block_force_partial(Fx, Fy, Fz, link, a.part);
+  warp_force_partial(Fx, Fy, Fz, near_cell, a);
 }
 
 }  // namespace wt

@@ -31,6 +31,7 @@ FLUID, SOLID_OBJ, SOLID_WALL = W.WT_FLUID, W.WT_SOLID_OBJ, W.WT_SOLID_WALL
 STORAGE = {"f32": W.WT_STORE_F32, "f16dev": W.WT_STORE_F16DEV, "f64": W.WT_STORE_F64}
 MATH = {"fast": W.WT_MATH_FAST, "exact": W.WT_MATH_EXACT}
 SIDE = {"eq": W.WT_SIDE_EQ, "freeslip": W.WT_SIDE_FREESLIP}
+KERNEL = {"auto": W.WT_KERNEL_AUTO, "direct": W.WT_KERNEL_DIRECT, "staged": W.WT_KERNEL_STAGED}
 _STORE_DTYPE = {W.WT_STORE_F32: np.float32, W.WT_STORE_F16DEV: np.float16,
                 W.WT_STORE_F64: np.float64}
 
@@ -65,7 +66,7 @@ class LBM:
     SOLID_WALL = SOLID_WALL
 
     def __init__(self, nx: int, ny: int, nz: int, storage: str = "f32", math: str = "fast",
-                 side_bc: str = "eq"):
+                 side_bc: str = "eq", kernel: str = "auto"):
         if storage not in STORAGE:
             raise ValueError(f"storage must be one of {sorted(STORAGE)}")
         L = lib()
@@ -78,6 +79,7 @@ class LBM:
         self._p = W.default_params()
         self._p.math = MATH[math]
         self._p.side_bc = SIDE[side_bc]
+        self._p.kernel = KERNEL[kernel]
         self._push()
         self._fields_at = -1
         self._fields = None
@@ -135,6 +137,7 @@ class LBM:
     movingWalls = _param("moving_walls", bool)
     side_bc = _param("side_bc", int)
     math = _param("math", int)
+    kernel = _param("kernel", int)
     del _param
 
     @property
@@ -159,6 +162,8 @@ class LBM:
                 v = SIDE[v]
             if key == "math" and isinstance(v, str):
                 v = MATH[v]
+            if key == "kernel" and isinstance(v, str):
+                v = KERNEL[v]
             cur = getattr(self._p, key)
             setattr(self._p, key, float(v) if isinstance(cur, float) else int(v))
         try:
