@@ -374,6 +374,7 @@ def run_wt(args) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": wl["name"], "lattice": [wl["nx"], wl["ny"], wl["nz"]],
                    "cells": n, "storage": "f32", "collision": "float32 (WT_MATH_FAST)",
+                   "kernel": "direct (one thread per cell, WT_KERNEL_AUTO)",
                    "tau": wl["tau"], "u0": wl["u0"], "les_cs": wl["csm"], "trt_lambda": wl["lam"],
                    "side_bc": wl["side_bc"],
                    "l2": "inputs larger than L2: two 318.8 MB population buffers per replica",

@@ -72,10 +72,14 @@ enum {
 
 /* Which step kernel runs. */
 enum {
-  WT_KERNEL_AUTO = 0,    /* staged when nx allows 16-byte aligned rows, else direct */
+  WT_KERNEL_AUTO = 0,    /* the kernel measured fastest on B200 for the form: direct */
   WT_KERNEL_DIRECT = 1,  /* one thread per cell, populations gathered straight from HBM */
-  WT_KERNEL_STAGED = 2   /* persistent CTAs staging the 19 pull rows with bulk copies (TMA);
+  WT_KERNEL_STAGED = 2,  /* persistent CTAs staging the 19 pull rows with bulk copies (TMA);
                             needs nx to be a multiple of 16 bytes / element size */
+  WT_KERNEL_VECTOR = 3,  /* two cells per thread, paired vector loads and stores with warp
+                            shuffles for the x-shifted directions; float32 collision, nx even */
+  WT_KERNEL_PIPE = 4     /* one thread per cell for 8 z planes, the next cell's loads issued
+                            before the current cell's collision; float32 collision */
 };
 
 /* Occupancy codes, js/lbm.js:39. */

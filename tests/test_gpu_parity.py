@@ -34,6 +34,8 @@ STAGE_VEC = {"f32": 4, "f16dev": 8, "f64": 2}   # nx must be a multiple for the 
 def kernel_or_skip(kernel, nx, storage="f32"):
     if kernel == "staged" and nx % STAGE_VEC[storage]:
         pytest.skip(f"staged kernel needs nx % {STAGE_VEC[storage]} == 0")
+    if kernel == "vector" and nx % 2:
+        pytest.skip("vector kernel needs an even nx")
     return kernel
 
 
@@ -128,7 +130,7 @@ def test_exact_cfg0_shape_bit_identical(both, kernel):
     assert_bit_exact(g, o, np.float32)
 
 
-@pytest.mark.parametrize("kernel", ["direct", "staged"])
+@pytest.mark.parametrize("kernel", ["direct", "staged", "vector", "pipe"])
 @pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
 def test_fast_f32_within_tolerance(both, side_bc, kernel):
     g, o = make_pair(both, (48, 24, 24), "f32", "fast", kernel=kernel,
@@ -177,7 +179,7 @@ def test_fast_cfg0_drag_and_fields(both):
     assert abs(clg - clo) <= 1e-3 * abs(cdo), (clg, clo)
 
 
-@pytest.mark.parametrize("kernel", ["direct", "staged"])
+@pytest.mark.parametrize("kernel", ["direct", "staged", "vector", "pipe"])
 def test_f16dev_within_tolerance(both, kernel):
     g, o = make_pair(both, (48, 24, 24), "f16dev", "fast", kernel=kernel,
                      sphere=(14.0, 12.0, 12.0, 5.0))
@@ -190,12 +192,13 @@ def test_f16dev_within_tolerance(both, kernel):
     assert abs(cg - co) <= 1e-2 * abs(co)
 
 
-@pytest.mark.parametrize("math", ["fast", "exact"])
+@pytest.mark.parametrize("math,kernel", [("fast", "direct"), ("fast", "vector"),
+                                         ("fast", "pipe"), ("exact", "direct")])
 @pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
-def test_uniform_flow_is_preserved(both, math, side_bc):
+def test_uniform_flow_is_preserved(both, math, kernel, side_bc):
     """A uniform stream past no body is a fixed point of the step (free-slip exactly)."""
     LBM, _ = both
-    s = LBM(20, 12, 10, math=math, side_bc=side_bc)
+    s = LBM(20, 12, 10, math=math, side_bc=side_bc, kernel=kernel)
     s.set_params(u0=0.05, tau=0.512)
     s.reset()
     s.step_forces(25)
@@ -221,21 +224,26 @@ def test_batch_equals_single_steps(both):
     assert np.array_equal(a.populations("f", "raw"), b.populations("f", "raw"))
 
 
+@pytest.mark.parametrize("dims", [(64, 20, 18), (38, 12, 10), (130, 9, 9), (40, 11, 21)])
 @pytest.mark.parametrize("storage", ["f32", "f16dev"])
-def test_staged_matches_direct(both, storage):
-    """Both kernels move the same values; the fast collision may round differently only
-    where the compiler contracts a multiply-add differently, so compare to 1e-6."""
+def test_kernels_agree(both, storage, dims):
+    """All three kernels move the same values; the fast collision may round
+    differently only where the compiler contracts a multiply-add differently."""
     LBM, _ = both
+    nx = dims[0]
+    kernels = ["direct", "vector", "pipe"] + (["staged"] if nx % STAGE_VEC[storage] == 0 else [])
     sims = []
-    for kernel in ("direct", "staged"):
-        s = LBM(64, 20, 18, storage=storage, kernel=kernel, side_bc="freeslip")
-        apply_case(s, sphere=(20.0, 9.0, 9.0, 4.5), side_bc="freeslip", ground=True,
-                   roadVel=0.02)
-        sims.append((s.step_forces(30), s.fields()))
-    (fa, ua), (fb, ub) = sims
-    assert np.abs(fa - fb).max() <= 1e-5 * np.abs(fa).max()
-    for a, b in zip(ua, ub):
-        assert np.abs(a - b).max() <= 1e-6
+    for kernel in kernels:
+        s = LBM(*dims, storage=storage, kernel=kernel, side_bc="freeslip")
+        apply_case(s, sphere=(nx - 6.0, dims[1] / 2, dims[2] / 2, 3.1), side_bc="freeslip",
+                   ground=True, roadVel=0.02)
+        sims.append((s.step_forces(30), s.fields(), s.populations("f", "f32")))
+    fa, ua, pa = sims[0]
+    for fb, ub, pb in sims[1:]:
+        assert np.abs(fa - fb).max() <= 1e-5 * np.abs(fa).max()
+        for a, b in zip(ua, ub):
+            assert np.abs(a - b).max() <= 1e-6
+        assert np.abs(pa - pb).max() <= (1e-6 if storage == "f32" else 1e-4)
 
 
 def test_step_is_deterministic(both):

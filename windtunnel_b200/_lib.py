@@ -36,6 +36,8 @@ WT_SIDE_FREESLIP = 1
 WT_KERNEL_AUTO = 0
 WT_KERNEL_DIRECT = 1
 WT_KERNEL_STAGED = 2
+WT_KERNEL_VECTOR = 3
+WT_KERNEL_PIPE = 4
 
 WT_FLUID = 0
 WT_SOLID_OBJ = 1

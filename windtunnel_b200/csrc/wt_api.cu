@@ -67,7 +67,7 @@ long long range_cells(const int rg[6]) {
 }
 
 void free_all(wt_lattice* h) {
-  void* dev[] = {h->buf[0], h->buf[1], h->flags, h->ux, h->uy, h->uz, h->rho, h->uwx, h->uwy,
+  void* dev[] = {h->buf[0], h->buf[1], h->flags, h->nmask, h->ux, h->uy, h->uz, h->rho, h->uwx, h->uwy,
                  h->uwz, h->part, h->wslot, h->forces_dev, h->err_dev, h->diag_dev, h->col,
                  h->plan, h->low, h->counters};
   for (void* p : dev)
@@ -83,9 +83,7 @@ int check_params(const wt_params* p) {
   if (p->trt && !(p->lambda > 0)) return WT_ERR_ARG;
   if (p->side_bc != WT_SIDE_EQ && p->side_bc != WT_SIDE_FREESLIP) return WT_ERR_ARG;
   if (p->math != WT_MATH_FAST && p->math != WT_MATH_EXACT) return WT_ERR_ARG;
-  if (p->kernel != WT_KERNEL_AUTO && p->kernel != WT_KERNEL_DIRECT &&
-      p->kernel != WT_KERNEL_STAGED)
-    return WT_ERR_ARG;
+  if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_PIPE) return WT_ERR_ARG;
   return WT_OK;
 }
 
@@ -118,6 +116,7 @@ template <class S>
 wt::StepArgs<S> make_args(wt_lattice* h) {
   wt::StepArgs<S> a{};
   a.flags = h->flags;
+  a.nmask = h->nmask;
   a.ux = h->ux; a.uy = h->uy; a.uz = h->uz; a.rho = h->rho;
   a.uwx = h->uwx; a.uwy = h->uwy; a.uwz = h->uwz;
   a.wslot = h->wslot;
@@ -146,8 +145,6 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
   a.trt = p.trt ? 1 : 0;
   a.mov = p.moving_walls ? 1 : 0;
   a.freeslip = p.side_bc == WT_SIDE_FREESLIP ? 1 : 0;
-  a.gx = (h->nx + wt::STEP_BX - 1) / wt::STEP_BX;
-  a.units = (long long)a.gx * h->ny * h->nz;
   double eq[19];
   wt::eq_u0_table(p.u0, eq);
   for (int q = 0; q < 19; q++) a.eq[q] = to_store<S>(eq[q]);
@@ -158,8 +155,11 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
 // direction block starts on a 16-byte boundary.
 bool staged_ok(const wt_lattice* h) { return h->nx % (int)(16 / h->elem) == 0; }
 
-template <class S, class L, class LS>
-void run_steps(wt_lattice* h, int nsteps, bool staged, L launch, LS launch_staged) {
+enum class Path { Direct, Staged, Vector, Pipe };
+
+template <class S, class L, class LS, class LV, class LP>
+void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged, LV launch_vec,
+               LP launch_pipe) {
   wt::StepArgs<S> a = make_args<S>(h);
   const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
   const bool wide = 19 * h->n >= (1LL << 31);
@@ -171,8 +171,12 @@ void run_steps(wt_lattice* h, int nsteps, bool staged, L launch, LS launch_stage
       a.G = (S*)h->buf[h->parity ^ 1];
       a.part = h->part + (size_t)s * stride;
       a.write_fields = (done + s == nsteps - 1) ? 1 : 0;
-      if (staged) launch_staged(a, h->stream);
-      else launch(a, grid, wide, h->stream);
+      switch (path) {
+        case Path::Staged: launch_staged(a, h->stream); break;
+        case Path::Vector: launch_vec(a, wide, h->stream); break;
+        case Path::Pipe: launch_pipe(a, wide, h->stream); break;
+        default: launch(a, grid, wide, h->stream); break;
+      }
       h->launches++;
       h->parity ^= 1;
     }
@@ -183,16 +187,21 @@ void run_steps(wt_lattice* h, int nsteps, bool staged, L launch, LS launch_stage
   }
 }
 
-// Assign a force-partial slot to every step-grid warp that holds a near-wall
-// cell (js/lbm.js:334-359 only accumulates there) and size the partial buffer.
+// No vector / pipe kernel exists for the float64 collision; this stands in their slots.
+template <class S>
+void no_vec(const wt::StepArgs<S>&, bool, cudaStream_t) {}
+
+// Assign a force-partial slot to every 32-cell segment that holds a
+// near-wall cell (js/lbm.js:334-359 only accumulates there) and size the
+// partial buffer.
 int rebuild_slots(wt_lattice* h) {
   uint8_t* mark = nullptr;
-  if (cudaMalloc(&mark, (size_t)h->nwarps) != cudaSuccess)
+  if (cudaMalloc(&mark, (size_t)h->nsegs) != cudaSuccess)
     return fail(h, WT_ERR_OOM, "cannot allocate the warp marks");
-  std::vector<uint8_t> hm((size_t)h->nwarps);
-  cudaError_t e = cudaMemsetAsync(mark, 0, (size_t)h->nwarps, h->stream);
+  std::vector<uint8_t> hm((size_t)h->nsegs);
+  cudaError_t e = cudaMemsetAsync(mark, 0, (size_t)h->nsegs, h->stream);
   if (e == cudaSuccess) {
-    wt::launch_mark_warps(h->flags, h->nx, h->ny, h->nz, mark, h->stream);
+    wt::launch_mark_segments(h->flags, h->nx, h->ny, h->nz, mark, h->stream);
     h->launches++;
     e = cudaMemcpyAsync(hm.data(), mark, hm.size(), cudaMemcpyDeviceToHost, h->stream);
   }
@@ -268,16 +277,16 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
   wt_default_params(&h->p);
   h->stats.frontal_area = 1;
   cudaGetDevice(&h->device);
-  const dim3 grid = wt::step_grid(nx, ny, nz);
-  h->nwarps = (long long)grid.x * grid.y * grid.z * wt::STEP_WARPS;
+  h->nsegs = (long long)((nx + 31) / 32) * ny * nz;
   const size_t pop = (size_t)n * 19 * h->elem;
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaMalloc(&h->buf[0], pop) == cudaSuccess;
   ok = ok && cudaMalloc(&h->buf[1], pop) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->flags, (size_t)n) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->nmask, sizeof(unsigned long long) * (size_t)n) == cudaSuccess;
   float** fl[] = {&h->ux, &h->uy, &h->uz, &h->rho, &h->uwx, &h->uwy, &h->uwz};
   for (float** p : fl) ok = ok && cudaMalloc((void**)p, sizeof(float) * (size_t)n) == cudaSuccess;
-  ok = ok && cudaMalloc((void**)&h->wslot, sizeof(int) * (size_t)h->nwarps) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&h->wslot, sizeof(int) * (size_t)h->nsegs) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->err_dev, sizeof(unsigned)) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->diag_dev, 4 * sizeof(long long)) == cudaSuccess;
   ok = ok && cudaMallocHost((void**)&h->err_host, sizeof(unsigned)) == cudaSuccess;
@@ -295,6 +304,7 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
     return WT_ERR_OOM;
   }
   cudaMemsetAsync(h->flags, 0, (size_t)n, h->stream);
+  cudaMemsetAsync(h->nmask, 0, sizeof(unsigned long long) * (size_t)n, h->stream);
   for (float* p : {h->uwx, h->uwy, h->uwz}) cudaMemsetAsync(p, 0, sizeof(float) * n, h->stream);
   wt::launch_init(h, 0, 0, 0);
   cudaError_t e = cudaStreamSynchronize(h->stream);
@@ -511,21 +521,47 @@ int wt_step(wt_lattice* h, int nsteps, double* forces) {
   if (c != WT_OK) return c;
   WT_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(unsigned), h->stream));
   WT_CUDA(h, cudaMemsetAsync(h->diag_dev, 0, 4 * sizeof(long long), h->stream));
-  const bool exact = h->p.math == WT_MATH_EXACT;
-  bool staged = staged_ok(h) && h->p.kernel != WT_KERNEL_DIRECT;
-  if (h->p.kernel == WT_KERNEL_STAGED && !staged_ok(h))
-    return fail(h, WT_ERR_UNSUPPORTED, "the staged kernel needs nx to be a multiple of " +
-                                           std::to_string(16 / h->elem));
-  switch (h->storage) {
-    case WT_STORE_F32:
-      if (exact) run_steps<float>(h, nsteps, staged, wt::launch_step_f32_exact, wt::launch_staged_f32_exact);
-      else run_steps<float>(h, nsteps, staged, wt::launch_step_f32_fast, wt::launch_staged_f32_fast);
+  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
+  const bool vec_ok = !exact && h->nx % 2 == 0;
+  Path path = Path::Direct;
+  switch (h->p.kernel) {
+    case WT_KERNEL_STAGED:
+      if (!staged_ok(h))
+        return fail(h, WT_ERR_UNSUPPORTED, "the staged kernel needs nx to be a multiple of " +
+                                               std::to_string(16 / h->elem));
+      path = Path::Staged;
       break;
-    case WT_STORE_F16DEV:
-      run_steps<__half>(h, nsteps, staged, wt::launch_step_f16_fast, wt::launch_staged_f16_fast);
+    case WT_KERNEL_VECTOR:
+      if (!vec_ok)
+        return fail(h, WT_ERR_UNSUPPORTED,
+                    "the vector kernel needs the float32 collision and an even nx");
+      path = Path::Vector;
+      break;
+    case WT_KERNEL_PIPE:
+      if (exact)
+        return fail(h, WT_ERR_UNSUPPORTED, "the pipe kernel runs the float32 collision only");
+      path = Path::Pipe;
+      break;
+    case WT_KERNEL_AUTO:   // the fastest measured on B200 for every form
+      path = Path::Direct;
       break;
     default:
-      run_steps<double>(h, nsteps, staged, wt::launch_step_f64_exact, wt::launch_staged_f64_exact);
+      break;
+  }
+  switch (h->storage) {
+    case WT_STORE_F32:
+      if (exact) run_steps<float>(h, nsteps, path, wt::launch_step_f32_exact,
+                                  wt::launch_staged_f32_exact, no_vec<float>, no_vec<float>);
+      else run_steps<float>(h, nsteps, path, wt::launch_step_f32_fast, wt::launch_staged_f32_fast,
+                            wt::launch_vec_f32, wt::launch_pipe_f32);
+      break;
+    case WT_STORE_F16DEV:
+      run_steps<__half>(h, nsteps, path, wt::launch_step_f16_fast, wt::launch_staged_f16_fast,
+                        wt::launch_vec_f16, wt::launch_pipe_f16);
+      break;
+    default:
+      run_steps<double>(h, nsteps, path, wt::launch_step_f64_exact, wt::launch_staged_f64_exact,
+                        no_vec<double>, no_vec<double>);
       break;
   }
   WT_CUDA(h, cudaGetLastError());
@@ -730,6 +766,8 @@ int wt_set_state(wt_lattice* h, const void* in, size_t bytes) {
   memcpy(h->force, hd.force, sizeof(hd.force));
   h->p = hd.params;
   h->stats = hd.stats;
+  wt::launch_near(h);   // near flags and neighbour masks follow from the restored occupancy
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
   return rebuild_slots(h);
 }
 

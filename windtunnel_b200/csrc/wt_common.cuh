@@ -103,6 +103,7 @@ struct StepArgs {
   const S* F;          // populations read (current f)
   S* G;                // populations written (next f)
   const uint8_t* flags;
+  const unsigned long long* nmask;  // per near-wall cell: solid neighbours (bits q), body (bits 32+q)
   float* ux;
   float* uy;
   float* uz;
@@ -137,10 +138,13 @@ inline dim3 step_grid(int nx, int ny, int nz) {
   return dim3((unsigned)((nx + STEP_BX - 1) / STEP_BX), (unsigned)ny, (unsigned)nz);
 }
 
-// Warp of the step grid that holds cell (x, y, z).
-__host__ __device__ inline long long step_warp_of(int x, int y, int z, int nx, int ny) {
-  const int gx = (nx + STEP_BX - 1) / STEP_BX;
-  return (((long long)z * ny + y) * gx + x / STEP_BX) * STEP_WARPS + (x % STEP_BX) / 32;
+// Force-partial segment of cell (x, y, z): 32 consecutive cells of a row.
+// Every step kernel reduces its momentum exchange per segment, so one slot
+// table (built by voxelize for the segments holding a near-wall cell) serves
+// them all.
+__host__ __device__ inline long long seg_of(int x, int y, int z, int nx, int ny) {
+  const int nseg = (nx + 31) / 32;
+  return ((long long)z * ny + y) * nseg + x / 32;
 }
 
 }  // namespace wt

@@ -20,6 +20,7 @@ struct wt_lattice {
   void* buf[2] = {nullptr, nullptr};  // population buffers A and B (js/lbm.js:74-75)
   int parity = 0;                // js/lbm.js:80: f = parity ? B : A
   uint8_t* flags = nullptr;      // solid code (bits 0-1) | near bit (bit 2)
+  unsigned long long* nmask = nullptr;  // near-wall cells: solid / body neighbour bits
   float* ux = nullptr;
   float* uy = nullptr;
   float* uz = nullptr;
@@ -27,10 +28,10 @@ struct wt_lattice {
   float* uwx = nullptr;          // wall velocities of solid cells (js/lbm.js:92-94)
   float* uwy = nullptr;
   float* uwz = nullptr;
-  // per-step force reduction: one partial per warp that holds a near-wall cell
-  long long nwarps = 0;          // warps of one step launch
-  int* wslot = nullptr;          // per warp: partial slot or -1
-  int nslots = 0;                // warps with a slot
+  // per-step force reduction: one partial per 32-cell segment holding a near-wall cell
+  long long nsegs = 0;           // 32-cell row segments of the lattice
+  int* wslot = nullptr;          // per segment: partial slot or -1
+  int nslots = 0;                // segments with a slot
   int part_cap = 0;              // slots that fit in `part` (per step of a chunk)
   double* part = nullptr;
   double* forces_dev = nullptr;
@@ -62,6 +63,14 @@ void launch_step_f16_fast(const StepArgs<__half>& a, dim3 grid, bool wide, cudaS
 void launch_step_f32_exact(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
 void launch_step_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cudaStream_t s);
 
+// Vector (two cells per thread) step launchers, float32 collision; nx even.
+void launch_vec_f32(const StepArgs<float>& a, bool wide, cudaStream_t s);
+void launch_vec_f16(const StepArgs<__half>& a, bool wide, cudaStream_t s);
+
+// Software-pipelined step launchers, float32 collision.
+void launch_pipe_f32(const StepArgs<float>& a, bool wide, cudaStream_t s);
+void launch_pipe_f16(const StepArgs<__half>& a, bool wide, cudaStream_t s);
+
 // Staged (bulk-copy) step launchers; need nx % (16 / sizeof(S)) == 0.
 void launch_staged_f32_fast(const StepArgs<float>& a, cudaStream_t s);
 void launch_staged_f16_fast(const StepArgs<__half>& a, cudaStream_t s);
@@ -72,9 +81,9 @@ void launch_staged_f64_exact(const StepArgs<double>& a, cudaStream_t s);
 void launch_force_reduce(const double* part, unsigned nslots, int nsteps, double* out,
                          cudaStream_t s);
 
-// mark[w] = 1 for every step-grid warp w holding a near-wall cell.
-void launch_mark_warps(const uint8_t* flags, int nx, int ny, int nz, uint8_t* mark,
-                       cudaStream_t s);
+// mark[s] = 1 for every 32-cell segment s holding a near-wall cell.
+void launch_mark_segments(const uint8_t* flags, int nx, int ny, int nz, uint8_t* mark,
+                          cudaStream_t s);
 
 // Equilibrium initialisation of both buffers and the fields:
 // mode 0 = reset(), mode 1 = reset() + seeded noise.

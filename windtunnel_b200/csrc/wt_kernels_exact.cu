@@ -227,23 +227,30 @@ __global__ void k_box(S* f, uint8_t* flags, Fields fl, Walls w, BoxStats st, int
 
 // js/lbm.js:268-282 (_rebuildNear): interior fluid cells with any solid
 // neighbour (object or wall) along the 18 moving directions.
-__global__ void k_near(uint8_t* flags, int nx, int ny, int nz, long long n) {
+// Also records, per near-wall cell, which of its 18 neighbours are solid
+// (bits 0-18) and which of those belong to the body (bits 32-50), so the step
+// can apply every bounce-back link of a cell after a single 8-byte load.
+__global__ void k_near(uint8_t* flags, unsigned long long* nmask, int nx, int ny, int nz,
+                       long long n) {
   const long long nxy = (long long)nx * ny;
   for (long long i = gtid(); i < n; i += gstride()) {
     const int x = (int)(i % nx);
     const int y = (int)((i / nx) % ny);
     const int z = (int)(i / nxy);
     const uint8_t v = flags[i];
-    bool near_cell = false;
+    unsigned long long m = 0;
     if (x >= 1 && x < nx - 1 && y >= 1 && y < ny - 1 && z >= 1 && z < nz - 1 &&
         !(v & FLAG_SOLID_MASK)) {
 #pragma unroll
       for (int q = 1; q < Q; q++) {
         const long long j = i - (ex(q) + (long long)ey(q) * nx + (long long)ez(q) * nxy);
-        if (flags[j] & FLAG_SOLID_MASK) near_cell = true;
+        const int sj = flags[j] & FLAG_SOLID_MASK;
+        if (sj) m |= 1ULL << q;
+        if (sj == WT_SOLID_OBJ) m |= 1ULL << (32 + q);
       }
     }
-    const uint8_t nv = (uint8_t)((v & FLAG_SOLID_MASK) | (near_cell ? FLAG_NEAR : 0));
+    nmask[i] = m;
+    const uint8_t nv = (uint8_t)((v & FLAG_SOLID_MASK) | (m ? FLAG_NEAR : 0));
     if (nv != v) flags[i] = nv;
   }
 }
@@ -365,7 +372,8 @@ void launch_box_grid(wt_lattice* h, const int rg[6], const uint8_t* grid_dev, in
 }
 
 void launch_near(wt_lattice* h) {
-  k_near<<<aux_blocks(h->n), AUX_T, 0, h->stream>>>(h->flags, h->nx, h->ny, h->nz, h->n);
+  k_near<<<aux_blocks(h->n), AUX_T, 0, h->stream>>>(h->flags, h->nmask, h->nx, h->ny, h->nz,
+                                                     h->n);
   h->launches++;
 }
 

@@ -3,6 +3,8 @@
 // the default multiply-add contraction.
 #include "wt_internal.h"
 #include "wt_staged_launch.cuh"
+#include "wt_pipe.cuh"
+#include "wt_vec.cuh"
 
 namespace wt {
 
@@ -16,6 +18,30 @@ void launch_step_f16_fast(const StepArgs<__half>& a, dim3 grid, bool wide, cudaS
   else k_step<__half, false, int><<<grid, STEP_BX, 0, s>>>(a);
 }
 
+void launch_vec_f32(const StepArgs<float>& a, bool wide, cudaStream_t s) {
+  const dim3 g = vec_grid(a.nx, a.ny, a.nz);
+  if (wide) k_step_vec<float, long long><<<g, VEC_BX, 0, s>>>(a);
+  else k_step_vec<float, int><<<g, VEC_BX, 0, s>>>(a);
+}
+
+void launch_vec_f16(const StepArgs<__half>& a, bool wide, cudaStream_t s) {
+  const dim3 g = vec_grid(a.nx, a.ny, a.nz);
+  if (wide) k_step_vec<__half, long long><<<g, VEC_BX, 0, s>>>(a);
+  else k_step_vec<__half, int><<<g, VEC_BX, 0, s>>>(a);
+}
+
+void launch_pipe_f32(const StepArgs<float>& a, bool wide, cudaStream_t s) {
+  const dim3 g = pipe_grid(a.nx, a.ny, a.nz);
+  if (wide) k_step_pipe<float, long long><<<g, STEP_BX, 0, s>>>(a);
+  else k_step_pipe<float, int><<<g, STEP_BX, 0, s>>>(a);
+}
+
+void launch_pipe_f16(const StepArgs<__half>& a, bool wide, cudaStream_t s) {
+  const dim3 g = pipe_grid(a.nx, a.ny, a.nz);
+  if (wide) k_step_pipe<__half, long long><<<g, STEP_BX, 0, s>>>(a);
+  else k_step_pipe<__half, int><<<g, STEP_BX, 0, s>>>(a);
+}
+
 void launch_staged_f32_fast(const StepArgs<float>& a, cudaStream_t s) {
   launch_staged<float, false>(a, s);
 }
@@ -24,22 +50,22 @@ void launch_staged_f16_fast(const StepArgs<__half>& a, cudaStream_t s) {
   launch_staged<__half, false>(a, s);
 }
 
-// Marks the warps of the step grid that hold at least one near-wall cell.
-__global__ void k_mark_warps(const uint8_t* __restrict__ flags, int nx, int ny, int nz,
+// Marks the 32-cell segments that hold at least one near-wall cell.
+__global__ void k_mark_segments(const uint8_t* __restrict__ flags, int nx, int ny, int nz,
                              uint8_t* __restrict__ mark) {
   const long long n = (long long)nx * ny * nz;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     if (flags[i] & FLAG_NEAR) {
       const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long long)nx * ny));
-      mark[step_warp_of(x, y, z, nx, ny)] = 1;
+      mark[seg_of(x, y, z, nx, ny)] = 1;
     }
   }
 }
 
-void launch_mark_warps(const uint8_t* flags, int nx, int ny, int nz, uint8_t* mark,
-                       cudaStream_t s) {
-  k_mark_warps<<<148 * 16, 256, 0, s>>>(flags, nx, ny, nz, mark);
+void launch_mark_segments(const uint8_t* flags, int nx, int ny, int nz, uint8_t* mark,
+                          cudaStream_t s) {
+  k_mark_segments<<<148 * 16, 256, 0, s>>>(flags, nx, ny, nz, mark);
 }
 
 // One block per step; each thread sums a fixed strided subset of the warp

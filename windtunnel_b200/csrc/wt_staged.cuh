@@ -33,13 +33,11 @@ struct Staged {
   static constexpr int VEC = 16 / (int)sizeof(S); // elements per 16 bytes
   static constexpr int PAD = VEC;                 // margin each side of a staged row
   static constexpr int W = TX + 2 * PAD;          // staged elements per direction
-  static constexpr int D = sizeof(S) == 8 ? 3 : 4;  // input stages (prefetch depth)
+  static constexpr int D = sizeof(S) == 8 ? 2 : 3;  // input stages
   static constexpr size_t IN_BYTES = (size_t)D * Q * W * sizeof(S);
   static constexpr size_t SMEM = IN_BYTES + 2 * D * sizeof(unsigned long long);
   // register budget: CTAs per SM the kernel is compiled to keep resident
-  static constexpr int min_blocks(bool exact) {
-    return exact ? 2 : (sizeof(S) == 2 ? 5 : 4);
-  }
+  static constexpr int min_blocks(bool exact) { return exact ? 2 : 5; }
 };
 
 // ---- PTX wrappers ----------------------------------------------------------------
@@ -56,6 +54,16 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t byt
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                : "memory");
 }
+// One lane of the (converged) warp, chosen by the hardware.
+__device__ __forceinline__ bool elect_one() {
+  uint32_t pred = 0;
+  asm volatile(
+      "{\n .reg .b32 r;\n .reg .pred p;\n elect.sync r|p, 0xffffffff;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(pred));
+  return pred != 0;
+}
+
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
@@ -148,47 +156,54 @@ struct UnitPos {
 template <class S>
 __device__ __forceinline__ void issue_unit(const StepArgs<S>& a, const UnitPos& p, S* in_stage,
                                            uint32_t bar) {
+  // Executed by the whole producer warp with uniform values; one elected
+  // lane performs the barrier arrival and the copies.
   using C = Staged<S>;
   const bool interior = p.y >= 1 && p.y <= a.ny - 2 && p.z >= 1 && p.z <= a.nz - 2;
-  if (!interior) {
-    mbar_arrive_expect_tx(bar, 0);
-    return;
-  }
   const int x0 = p.tile * C::TX;
   const int w = min(C::TX, a.nx - x0);
   const uint32_t bytes = (uint32_t)((w + 2 * C::PAD) * sizeof(S));
   const long long rowbase = (long long)a.nx * p.y + a.nxy * p.z + x0 - C::PAD;
+  int bad = -1;
+  if (interior) {
 #pragma unroll
-  for (int q = 0; q < Q; q++) {
-    // the row of direction q, unshifted in x: the -ex shift is applied when
-    // the threads read the stage (index t + PAD - ex)
-    const long long off = a.src[q] + ex(q) + rowbase;
-    const uintptr_t sa = (uintptr_t)(a.F + off);
-    if (sa % 16 != 0 || off < 0 || off + (w + 2 * C::PAD) > 19 * a.n) {
-      report_copy(a, 1, q, p.u, off);   // would leave its buffer or be misaligned: skip the unit
-      mbar_arrive_expect_tx(bar, 0);
-      return;
+    for (int q = 0; q < Q; q++) {
+      // the row of direction q, unshifted in x: the -ex shift is applied when
+      // the threads read the stage (index t + PAD - ex)
+      const long long off = a.src[q] + ex(q) + rowbase;
+      if ((uintptr_t)(a.F + off) % 16 != 0 || off < 0 || off + (w + 2 * C::PAD) > 19 * a.n)
+        bad = q;
     }
   }
-  mbar_arrive_expect_tx(bar, bytes * Q);
+  if (elect_one()) {
+    if (!interior) {
+      mbar_arrive_expect_tx(bar, 0);
+    } else if (bad >= 0) {
+      report_copy(a, 1, bad, p.u, a.src[bad] + ex(bad) + rowbase);   // skipped, reported
+      mbar_arrive_expect_tx(bar, 0);
+    } else {
+      mbar_arrive_expect_tx(bar, bytes * Q);
 #pragma unroll
-  for (int q = 0; q < Q; q++) {
-    bulk_g2s(smem_addr(in_stage + q * C::W), a.F + a.src[q] + ex(q) + rowbase, bytes, bar);
+      for (int q = 0; q < Q; q++) {
+        bulk_g2s(smem_addr(in_stage + q * C::W), a.F + a.src[q] + ex(q) + rowbase, bytes, bar);
+      }
+    }
   }
+  __syncwarp();
 }
 
 // Writer of the collision outputs straight to HBM (the staged kernel's
-// stores): direction q of cell i goes to base[dst[q]].
+// stores): direction q of cell i goes to base[q * n].
 template <class S, class IDX>
 struct GlobalOut {
   S* base;                   // G + i
-  const long long* dst;      // per-direction store offsets (kernel parameters)
-  __device__ __forceinline__ void put(int q, S v) { base[(IDX)dst[q]] = v; }
+  IDX n;                     // cells per direction block
+  __device__ __forceinline__ void put(int q, S v) { base[(IDX)q * n] = v; }
 };
 
 template <class S, bool EXACT, class IDX>
 __global__ void __launch_bounds__(Staged<S>::THREADS, Staged<S>::min_blocks(EXACT))
-    k_step_staged(const StepArgs<S> a) {
+    k_step_staged(const __grid_constant__ StepArgs<S> a) {
   using C = Staged<S>;
   using M = typename std::conditional<EXACT, double, float>::type;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -214,20 +229,18 @@ __global__ void __launch_bounds__(Staged<S>::THREADS, Staged<S>::min_blocks(EXAC
   __syncthreads();
 
   if (warp == C::NCONS) {
-    // ---- producer: one lane issues every unit's 19 row copies -------------------
-    if (lane == 0) {
-      UnitPos pf;
-      pf.start(ubeg, a.gx, a.ny);
-      for (long long k = 0; k < count; k++, pf.next(a.gx, a.ny)) {
-        const int stage = (int)(k % C::D);
-        if (k >= C::D &&
-            !mbar_wait_bounded(smem_addr(&empty[stage]), (uint32_t)((k / C::D - 1) & 1),
-                               kWaitBudgetCycles)) {
-          atomicOr(a.err, 4u);   // consumers stopped: issue nothing more
-          return;
-        }
-        issue_unit(a, pf, in_s + (size_t)stage * Q * C::W, smem_addr(&full[stage]));
+    // ---- producer warp: issues every unit's 19 row copies -------------------------
+    UnitPos pf;
+    pf.start(ubeg, a.gx, a.ny);
+    for (long long k = 0; k < count; k++, pf.next(a.gx, a.ny)) {
+      const int stage = (int)(k % C::D);
+      if (k >= C::D &&
+          !mbar_wait_bounded(smem_addr(&empty[stage]), (uint32_t)((k / C::D - 1) & 1),
+                             kWaitBudgetCycles)) {
+        if (lane == 0) atomicOr(a.err, 4u);   // consumers stopped: issue nothing more
+        return;
       }
+      issue_unit(a, pf, in_s + (size_t)stage * Q * C::W, smem_addr(&full[stage]));
     }
     return;
   }
@@ -237,7 +250,21 @@ __global__ void __launch_bounds__(Staged<S>::THREADS, Staged<S>::min_blocks(EXAC
   const int gx = a.gx, ny = a.ny, nz = a.nz, nx = a.nx;
   UnitPos p;
   p.start(ubeg, gx, ny);
+  // the occupancy byte of this thread's cell in the next unit is loaded one
+  // unit ahead, so its HBM round trip overlaps the current unit's collision
+  auto flag_of = [&](const UnitPos& q) -> uint8_t {
+    const int xq = q.tile * C::TX + t;
+    if (xq >= nx) return 0;
+    return a.flags[(long long)xq + (long long)nx * q.y + a.nxy * q.z];
+  };
+  uint8_t fl_next = flag_of(p);
   for (long long k = 0; k < count; k++, p.next(gx, ny)) {
+    const uint8_t fl_cur = fl_next;
+    if (k + 1 < count) {
+      UnitPos pn = p;
+      pn.next(gx, ny);
+      fl_next = flag_of(pn);
+    }
     const int stage = (int)(k % C::D);
     if (!mbar_wait_bounded(smem_addr(&full[stage]), (uint32_t)((k / C::D) & 1),
                            kWaitBudgetCycles)) {
@@ -262,7 +289,7 @@ __global__ void __launch_bounds__(Staged<S>::THREADS, Staged<S>::min_blocks(EXAC
       if (x == 0 || edge_row) {
         cat = CAT_EQ;
       } else {
-        fl = a.flags[i];
+        fl = fl_cur;
         if (fl & FLAG_SOLID_MASK) cat = CAT_KEEP;
         else if (y == 0) cat = CAT_EQ;
         else cat = CAT_FLUID;
@@ -276,9 +303,9 @@ __global__ void __launch_bounds__(Staged<S>::THREADS, Staged<S>::min_blocks(EXAC
         if (near_cell || shell) patch_special<S, M>(a, i, x, y, z, shell, f, Fx, Fy, Fz);
         if (!dup) {
           if constexpr (EXACT) {
-            collide_exact<S>(a, f, i, false, near_cell, GlobalOut<S, IDX>{Gi, a.dst});
+            collide_exact<S>(a, f, i, false, near_cell, GlobalOut<S, IDX>{Gi, (IDX)a.n});
           } else {
-            collide_fast<S>(a, f, i, false, near_cell, GlobalOut<S, IDX>{Gi, a.dst});
+            collide_fast<S>(a, f, i, false, near_cell, GlobalOut<S, IDX>{Gi, (IDX)a.n});
           }
         } else {
           S o[Q];
@@ -312,7 +339,8 @@ __global__ void __launch_bounds__(Staged<S>::THREADS, Staged<S>::min_blocks(EXAC
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_addr(&empty[stage]));
-    warp_force_partial_unit(Fx, Fy, Fz, near_cell, a, p.u);
+    warp_force_partial_w(Fx, Fy, Fz, near_cell, a,
+                         seg_of(x0 + (t & ~31), y, z, nx, ny));
   }
 }
 

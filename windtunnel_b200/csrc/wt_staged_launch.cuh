@@ -10,8 +10,11 @@ namespace wt {
 // Persistent grid: as many CTAs as fit on the device at once (cached per
 // device), never more than there are units.
 template <class S, bool EXACT, class IDX>
-void launch_staged_idx(const StepArgs<S>& a, cudaStream_t s) {
+void launch_staged_idx(const StepArgs<S>& args, cudaStream_t s) {
   using C = Staged<S>;
+  StepArgs<S> a = args;   // units are x-segments of C::TX cells
+  a.gx = (a.nx + C::TX - 1) / C::TX;
+  a.units = (long long)a.gx * a.ny * a.nz;
   constexpr int kMaxDevices = 64;
   static int grid_of[kMaxDevices] = {0};
   int dev = 0;

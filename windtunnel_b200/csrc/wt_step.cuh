@@ -45,16 +45,17 @@ struct TileOut {
 
 enum : int { CAT_NONE = 0, CAT_EQ = 1, CAT_KEEP = 2, CAT_FLUID = 3 };
 
-// Sum three doubles over the warp in a fixed order and store them in the
-// warp's partial slot. Exactly the warps that hold a near-wall cell own a slot
-// (the table is rebuilt by voxelize), and each of them writes its slot every
-// step -- zeros when none of its links touches the body -- so the ~all-fluid
-// warps write nothing and no block-wide barrier is needed. Every lane of the
-// warp must call it; `near_cell` marks a computed near-wall cell.
+// Sum three doubles over a warp that covers one 32-cell segment, in a fixed
+// order, and store them in the segment's partial slot. Exactly the segments
+// that hold a near-wall cell own a slot (the table is rebuilt by voxelize),
+// and each of them is written every step -- zeros when none of its links
+// touches the body -- so all-fluid warps write nothing and no block-wide
+// barrier is needed. Every lane of the warp must call it; `near_cell` marks a
+// computed near-wall cell.
 template <class S>
 __device__ __forceinline__ void warp_force_partial_w(double fx, double fy, double fz,
                                                      bool near_cell, const StepArgs<S>& a,
-                                                     long long warp_id) {
+                                                     long long seg) {
   if (__any_sync(0xffffffffu, near_cell)) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -63,7 +64,7 @@ __device__ __forceinline__ void warp_force_partial_w(double fx, double fy, doubl
       fz += __shfl_down_sync(0xffffffffu, fz, o);
     }
     if ((threadIdx.x & 31) == 0) {
-      const int slot = a.wslot[warp_id];
+      const int slot = a.wslot[seg];
       if (slot >= 0) {
         a.part[3 * (size_t)slot] = fx;
         a.part[3 * (size_t)slot + 1] = fy;
@@ -75,20 +76,12 @@ __device__ __forceinline__ void warp_force_partial_w(double fx, double fy, doubl
   }
 }
 
-// Warp partial of the direct kernel, whose block b covers unit b.
+// Warp partial of the direct kernel: its warps cover 32-cell segments.
 template <class S>
 __device__ __forceinline__ void warp_force_partial(double fx, double fy, double fz,
                                                    bool near_cell, const StepArgs<S>& a) {
-  const long long b = (long long)(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-  warp_force_partial_w(fx, fy, fz, near_cell, a, b * STEP_WARPS + (threadIdx.x >> 5));
-}
-
-// Warp partial of the staged kernel, processing unit u.
-template <class S>
-__device__ __forceinline__ void warp_force_partial_unit(double fx, double fy, double fz,
-                                                        bool near_cell, const StepArgs<S>& a,
-                                                        long long u) {
-  warp_force_partial_w(fx, fy, fz, near_cell, a, u * STEP_WARPS + (threadIdx.x >> 5));
+  const int x0 = blockIdx.x * STEP_BX + (threadIdx.x & ~31);
+  warp_force_partial_w(fx, fy, fz, near_cell, a, seg_of(x0, blockIdx.y, blockIdx.z, a.nx, a.ny));
 }
 
 // Bounce-back link q of cell i toward solid neighbour j (code s):
@@ -114,71 +107,33 @@ __device__ __forceinline__ M bounce_link(const StepArgs<S>& a, long long i, long
 
 // Overwrite, in f (already holding the plain pulled values), the directions
 // whose source is solid (bounce-back) or lies on a free-slip side plane
-// (mirror gather). Used by the staged kernel.
+// (mirror gather). The solid / body neighbours come from the cell's
+// precomputed mask (one load); the loads below depend only on it and on the
+// cell position, so they are all in flight at once.
 template <class S, class M>
 __device__ __forceinline__ void patch_special(const StepArgs<S>& a, long long i, int x, int y,
                                               int z, bool shell, M (&f)[Q], double& Fx,
                                               double& Fy, double& Fz) {
-  const M rho_prev = (M)(a.mov ? a.rho[i] : 1.0f);
-#define WT_PATCH(q)                                                                       \
-  {                                                                                       \
-    const long long j = i - (ex(q) + (long long)ey(q) * a.nx + (long long)ez(q) * a.nxy); \
-    const int s = a.flags[j] & FLAG_SOLID_MASK;                                           \
-    if (s) {                                                                              \
-      f[q] = bounce_link<S, M, q>(a, i, j, s, rho_prev, Fx, Fy, Fz);                      \
-    } else if (shell) {                                                                   \
-      int sy = y - ey(q), sz = z - ez(q), qq = q;                                         \
-      bool refl = false;                                                                  \
-      if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); refl = true; }          \
-      if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); refl = true; }          \
-      if (refl)                                                                           \
-        f[q] = ld<M>(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);    \
-    }                                                                                     \
+  const unsigned long long m = a.nmask[i];
+  const unsigned sm = (unsigned)m, om = (unsigned)(m >> 32);
+  const M rho_prev = (M)(a.mov && sm ? a.rho[i] : 1.0f);
+#define WT_PATCH(q)                                                                         \
+  if ((sm >> (q)) & 1u) {                                                                   \
+    const long long j = i - (ex(q) + (long long)ey(q) * a.nx + (long long)ez(q) * a.nxy);   \
+    f[q] = bounce_link<S, M, q>(a, i, j, ((om >> (q)) & 1u) ? WT_SOLID_OBJ : WT_SOLID_WALL, \
+                                rho_prev, Fx, Fy, Fz);                                      \
+  } else if (shell) {                                                                       \
+    int sy = y - ey(q), sz = z - ez(q), qq = q;                                             \
+    bool refl = false;                                                                      \
+    if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); refl = true; }              \
+    if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); refl = true; }              \
+    if (refl)                                                                               \
+      f[q] = ld<M>(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);        \
   }
   WT_PATCH(1) WT_PATCH(2) WT_PATCH(3) WT_PATCH(4) WT_PATCH(5) WT_PATCH(6) WT_PATCH(7)
   WT_PATCH(8) WT_PATCH(9) WT_PATCH(10) WT_PATCH(11) WT_PATCH(12) WT_PATCH(13) WT_PATCH(14)
   WT_PATCH(15) WT_PATCH(16) WT_PATCH(17) WT_PATCH(18)
 #undef WT_PATCH
-}
-
-// Gather for cells next to a solid (bounce-back + momentum exchange,
-// js/lbm.js:334-368) or next to a free-slip side plane (mirror gather).
-template <class S, class M>
-__device__ __forceinline__ void gather_special(const StepArgs<S>& a, long long i, int x, int y,
-                                               int z, bool shell, M (&f)[Q], double& Fx,
-                                               double& Fy, double& Fz) {
-  const long long n = a.n;
-  const M rho_prev = (M)(a.mov ? a.rho[i] : 1.0f);
-#pragma unroll
-  for (int q = 0; q < Q; q++) {
-    const long long off = ex(q) + (long long)ey(q) * a.nx + (long long)ez(q) * a.nxy;
-    const long long j = i - off;
-    const int s = q == 0 ? 0 : (a.flags[j] & FLAG_SOLID_MASK);
-    if (s) {
-      const M fd = ld<M>(a.F[opp(q) * n + i]);
-      M corr = 0;
-      if (a.mov) {
-        const M cu = (M)ex(q) * (M)a.uwx[j] + (M)ey(q) * (M)a.uwy[j] + (M)ez(q) * (M)a.uwz[j];
-        if (cu != (M)0) corr = (M)6 * (M)wq(q) * rho_prev * cu;
-      }
-      f[q] = fd + corr;
-      if (s == WT_SOLID_OBJ) {
-        const M d = (M)2 * fd + corr;
-        Fx -= (double)(d * (M)ex(q));
-        Fy -= (double)(d * (M)ey(q));
-        Fz -= (double)(d * (M)ez(q));
-      }
-    } else {
-      long long src = q * n + i - off;
-      if (shell) {
-        int sx = x - ex(q), sy = y - ey(q), sz = z - ez(q), qq = q;
-        if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); }
-        if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); }
-        src = qq * n + sx + (long long)a.nx * sy + a.nxy * sz;
-      }
-      f[q] = ld<M>(a.F[src]);
-    }
-  }
 }
 
 // Float32 collision, re-associated: opposite pairs are carried as half sums
@@ -351,7 +306,7 @@ constexpr int step_min_blocks(bool exact) { return exact ? 4 : 8; }
 // IDX is the type of the per-direction offsets: int when 19*n fits in 31
 // bits (every practical lattice), long long otherwise.
 template <class S, bool EXACT, class IDX>
-__global__ void __launch_bounds__(STEP_BX, step_min_blocks(EXACT)) k_step(const StepArgs<S> a) {
+__global__ void __launch_bounds__(STEP_BX, step_min_blocks(EXACT)) k_step(const __grid_constant__ StepArgs<S> a) {
   using M = typename std::conditional<EXACT, double, float>::type;
   const int x = blockIdx.x * STEP_BX + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
@@ -376,13 +331,10 @@ __global__ void __launch_bounds__(STEP_BX, step_min_blocks(EXACT)) k_step(const 
       M f[Q];
       near_cell = (fl & FLAG_NEAR) != 0;
       const bool shell = a.freeslip && (y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2);
-      if (near_cell || shell) {
-        gather_special<S, M>(a, i, x, y, z, shell, f, Fx, Fy, Fz);
-      } else {
-        const S* Fi = a.F + i;
+      const S* Fi = a.F + i;
 #pragma unroll
-        for (int q = 0; q < Q; q++) f[q] = ld<M>(Fi[(IDX)a.src[q]]);
-      }
+      for (int q = 0; q < Q; q++) f[q] = ld<M>(Fi[(IDX)a.src[q]]);
+      if (near_cell || shell) patch_special<S, M>(a, i, x, y, z, shell, f, Fx, Fy, Fz);
       S out[Q];
       if constexpr (EXACT) {
         collide_exact<S>(a, f, i, dup, near_cell, RegOut<S>{out});
