@@ -56,6 +56,11 @@ WORKLOADS = {
         side_bc="freeslip", body=dict(semi=(0.5, 0.1875, 0.15), exponent=2.5, res=160,
                                       scale=80.0, yaw_deg=15.0), seed=1234, amp=1e-4,
         accuracy_steps=10000, accuracy_window=2000),
+    "sphere128": dict(
+        name="128x64x64 D3Q19 channel, sphere r=8 at (32,32,32), Re=200",
+        nx=128, ny=64, nz=64, u0=0.05, tau=0.512, csm=0.1, lam=3 / 16, les=True,
+        side_bc="freeslip", sphere=(32.0, 32.0, 32.0, 8.0), seed=1234, amp=1e-4,
+        accuracy_steps=2000, accuracy_window=500),
     "channel512": dict(
         name="512x192x192 D3Q19 channel, yawed superellipsoid hull x2",
         nx=512, ny=192, nz=192, u0=0.06, tau=0.5072, csm=0.1, lam=3 / 16, les=True,
@@ -77,13 +82,16 @@ def body_inputs(wl):
 
 
 def setup_gpu(wl, storage, math_mode="fast"):
-    from windtunnel_b200 import LBM
+    from windtunnel_b200 import LBM, sphere_box, sphere_inside
     sim = LBM(wl["nx"], wl["ny"], wl["nz"], storage=storage, math=math_mode,
               side_bc=wl["side_bc"])
     sim.set_params(u0=wl["u0"], tau=wl["tau"], csm=wl["csm"], les=int(wl["les"]),
                    **{"lambda": wl["lam"]})
-    vg, M, P, box = body_inputs(wl)
-    sim.voxelize_grid(vg.grid, vg.min, vg.inv, M, P, wl["body"]["scale"], box)
+    if "sphere" in wl:
+        sim.voxelize(sphere_inside(*wl["sphere"]), sphere_box(*wl["sphere"]))
+    else:
+        vg, M, P, box = body_inputs(wl)
+        sim.voxelize_grid(vg.grid, vg.min, vg.inv, M, P, wl["body"]["scale"], box)
     sim.init_eq_noise(wl["seed"], wl["amp"])
     return sim
 
@@ -287,25 +295,53 @@ def pair_avg_coeff(forces, u0, area, window):
     return float(w[:, 0].mean() / q), float(w[:, 1].mean() / q)
 
 
-def accuracy_study(wl) -> dict:
-    """Cd / Cl of FP32, FP16-dev and FP64 storage after the workload's full step count."""
+def accuracy_study(wl, long_steps: int = 20000) -> dict:
+    """Cd / Cl of every storage form vs FP64, with blocking standard errors.
+
+    Each form runs the workload's step count and reports the pair-averaged
+    coefficients over its last `window` steps (the configuration's
+    statistic), then runs `long_steps` more and reports the average over
+    those as well, which separates a bias of the storage form from the
+    sampling noise of a turbulent wake.
+    """
+    from windtunnel_b200.stats import window_coefficients
     out = {"steps": wl["accuracy_steps"], "window": wl["accuracy_window"],
-           "average": "pair-averaged consecutive steps (js/main.js:113-127)"}
-    coeffs = {}
-    for storage, mm in (("f64", "exact"), ("f32", "fast"), ("f16dev", "fast")):
+           "long_window": long_steps,
+           "average": "pair-averaged consecutive steps (js/main.js:113-127), "
+                      "16-block blocking SEM (js/main.js:163-191)"}
+    res = {}
+    forms = (("f64", "f64", "exact", None), ("f32", "f32", "fast", None),
+             ("f16dev", "f16dev", "fast", "stochastic"),
+             ("f16dev_nearest", "f16dev", "fast", "nearest"))
+    for name, storage, mm, rounding in forms:
         sim = setup_gpu(wl, storage, mm)
+        if rounding:
+            sim.set_params(f16_rounding=rounding)
         t0 = time.time()
         F = sim.step_forces(wl["accuracy_steps"])
-        cd, cl = pair_avg_coeff(F, wl["u0"], sim.frontalArea, wl["accuracy_window"])
-        coeffs[storage] = (cd, cl)
-        out[storage] = {"cd": cd, "cl": cl, "wall_s": round(time.time() - t0, 2)}
+        short = window_coefficients(F, wl["u0"], sim.frontalArea, wl["accuracy_window"])
+        F2 = sim.step_forces(long_steps) if long_steps else None
+        entry = {"cd": short["cd"], "cd_sem": short["cd_sem"], "cl": short["cl"],
+                 "cl_sem": short["cl_sem"]}
+        if F2 is not None:
+            lw = window_coefficients(F2, wl["u0"], sim.frontalArea, long_steps - 1)
+            entry.update(cd_long=lw["cd"], cd_long_sem=lw["cd_sem"], cl_long=lw["cl"],
+                         cl_long_sem=lw["cl_sem"])
+        entry["wall_s"] = round(time.time() - t0, 2)
+        if rounding:
+            entry["rounding"] = rounding
+        res[name] = entry
         sim.close()
-    cd64 = coeffs["f64"][0]
-    for s in ("f32", "f16dev"):
-        out[s]["dcd_rel_vs_f64"] = abs(coeffs[s][0] - cd64) / abs(cd64)
-        out[s]["dcl_vs_f64_over_cd"] = abs(coeffs[s][1] - coeffs["f64"][1]) / abs(cd64)
-    out["f16dev"]["dcd_rel_vs_f32"] = abs(coeffs["f16dev"][0] - coeffs["f32"][0]) / abs(
-        coeffs["f32"][0])
+    ref = res["f64"]
+    for name, e in res.items():
+        if name == "f64":
+            continue
+        e["dcd_rel_vs_f64"] = abs(e["cd"] - ref["cd"]) / abs(ref["cd"])
+        if "cd_long" in e:
+            e["dcd_long_rel_vs_f64"] = abs(e["cd_long"] - ref["cd_long"]) / abs(ref["cd_long"])
+            e["dcd_long_sigma"] = abs(e["cd_long"] - ref["cd_long"]) / math.hypot(
+                e["cd_long_sem"], ref["cd_long_sem"])
+    out.update(res)
     return out
 
 
@@ -396,6 +432,7 @@ def run_wt(args) -> None:
     }
     if args.accuracy and dist.rank == 0:
         line["accuracy"] = accuracy_study(wl)
+        line["accuracy_steady"] = accuracy_study(WORKLOADS["sphere128"], long_steps=0)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl)
     dist.barrier()

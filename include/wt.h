@@ -82,6 +82,10 @@ enum {
                             before the current cell's collision; float32 collision */
 };
 
+/* Rounding of half-precision stores. Stochastic rounding draws its random
+ * bits from a hash of (cell, step), so a run is reproducible. */
+enum { WT_ROUND_NEAREST = 0, WT_ROUND_STOCHASTIC = 1 };
+
 /* Occupancy codes, js/lbm.js:39. */
 enum { WT_FLUID = 0, WT_SOLID_OBJ = 1, WT_SOLID_WALL = 2 };
 
@@ -100,7 +104,9 @@ typedef struct wt_params {
   int32_t moving_walls; /* moving no-slip walls on/off (LBM.movingWalls; set by voxelize) */
   int32_t side_bc;   /* WT_SIDE_EQ (default) or WT_SIDE_FREESLIP */
   int32_t math;      /* WT_MATH_FAST (default) or WT_MATH_EXACT */
-  int32_t kernel;    /* WT_KERNEL_AUTO (default), WT_KERNEL_DIRECT or WT_KERNEL_STAGED */
+  int32_t kernel;    /* WT_KERNEL_* (default WT_KERNEL_AUTO) */
+  int32_t f16_rounding; /* half storage: WT_ROUND_NEAREST or WT_ROUND_STOCHASTIC (default) */
+  int32_t reserved;  /* must be 0 */
 } wt_params;
 
 /* Body statistics computed by voxelize, js/lbm.js:247-264. */

@@ -78,6 +78,7 @@ void or_default_params(wt_params* p) {
   p->moving_walls = 0;
   p->side_bc = 0;
   p->math = 1;
+  p->f16_rounding = 1;
 }
 
 static int or_clamp_int(double v) {

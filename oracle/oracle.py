@@ -37,6 +37,7 @@ class wt_params(C.Structure):
         ("u0", C.c_double), ("tau", C.c_double), ("les", C.c_int32), ("trt", C.c_int32),
         ("csm", C.c_double), ("lambda_", C.c_double), ("moving_walls", C.c_int32),
         ("side_bc", C.c_int32), ("math", C.c_int32), ("kernel", C.c_int32),
+        ("f16_rounding", C.c_int32), ("reserved", C.c_int32),
     ]
 
 

@@ -39,6 +39,9 @@ WT_KERNEL_STAGED = 2
 WT_KERNEL_VECTOR = 3
 WT_KERNEL_PIPE = 4
 
+WT_ROUND_NEAREST = 0
+WT_ROUND_STOCHASTIC = 1
+
 WT_FLUID = 0
 WT_SOLID_OBJ = 1
 WT_SOLID_WALL = 2
@@ -69,6 +72,8 @@ class wt_params(C.Structure):
         ("side_bc", C.c_int32),
         ("math", C.c_int32),
         ("kernel", C.c_int32),
+        ("f16_rounding", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -84,6 +84,9 @@ int check_params(const wt_params* p) {
   if (p->side_bc != WT_SIDE_EQ && p->side_bc != WT_SIDE_FREESLIP) return WT_ERR_ARG;
   if (p->math != WT_MATH_FAST && p->math != WT_MATH_EXACT) return WT_ERR_ARG;
   if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_PIPE) return WT_ERR_ARG;
+  if (p->f16_rounding != WT_ROUND_NEAREST && p->f16_rounding != WT_ROUND_STOCHASTIC)
+    return WT_ERR_ARG;
+  if (p->reserved != 0) return WT_ERR_ARG;
   return WT_OK;
 }
 
@@ -145,6 +148,7 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
   a.trt = p.trt ? 1 : 0;
   a.mov = p.moving_walls ? 1 : 0;
   a.freeslip = p.side_bc == WT_SIDE_FREESLIP ? 1 : 0;
+  a.f16_sr = p.f16_rounding == WT_ROUND_STOCHASTIC ? 1 : 0;
   double eq[19];
   wt::eq_u0_table(p.u0, eq);
   for (int q = 0; q < 19; q++) a.eq[q] = to_store<S>(eq[q]);
@@ -171,6 +175,7 @@ void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged,
       a.G = (S*)h->buf[h->parity ^ 1];
       a.part = h->part + (size_t)s * stride;
       a.write_fields = (done + s == nsteps - 1) ? 1 : 0;
+      a.sr_seed = (unsigned)((uint64_t)(h->steps + done + s) * 0x9E3779B97F4A7C15ULL >> 32);
       switch (path) {
         case Path::Staged: launch_staged(a, h->stream); break;
         case Path::Vector: launch_vec(a, wide, h->stream); break;
@@ -244,6 +249,8 @@ void wt_default_params(wt_params* p) {
   p->moving_walls = 0;
   p->side_bc = WT_SIDE_EQ;
   p->math = WT_MATH_FAST;
+  p->kernel = WT_KERNEL_AUTO;
+  p->f16_rounding = WT_ROUND_STOCHASTIC;
 }
 
 const char* wt_last_error(const wt_lattice* h) {

@@ -125,6 +125,8 @@ struct StepArgs {
   // float32 parameters (fast collision), rounded once on the host
   float tau0f, omega0f, omm0f, les_cf, lamf, u0f;
   int les, trt, mov, freeslip, write_fields;
+  int f16_sr;          // half storage: stochastic instead of nearest rounding
+  unsigned sr_seed;    // per-step seed of the stochastic rounding
   int gx;              // x-segments (units) per row
   long long units;     // gx*ny*nz
   S eq[Q];             // equilibrium deviation at rho=1, u=(u0,0,0), rounded to S

@@ -29,6 +29,14 @@ __device__ __forceinline__ M ld(S v) {
   else return Store<S>::load_f(v);
 }
 
+// Stochastic rounding of two floats to a half pair (hi <- a, lo <- b) with
+// the random bits rbits (sm_100a cvt.rs).
+__device__ __forceinline__ __half2 sr_half2(float a, float b, uint32_t rbits) {
+  uint32_t d;
+  asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(a), "f"(b), "r"(rbits));
+  return *reinterpret_cast<__half2*>(&d);
+}
+
 // Output writers of the collision: into a register array (direct kernel) or
 // straight into a shared-memory output tile (staged kernel).
 template <class S>
@@ -201,13 +209,40 @@ __device__ __forceinline__ void collide_fast(const StepArgs<S>& a, const float (
     }
   }
   const float e0 = W0 * A;
-  out.put(0, Store<S>::from_f(fmaf(-om, f[0] - e0, f[0])));
-#define WT_OUT(k, kb)                                                          \
-  out.put(k, Store<S>::from_f(fmaf(-omm, sm##k, fmaf(-om, sp##k, f[k]))));     \
-  out.put(kb, Store<S>::from_f(fmaf(omm, sm##k, fmaf(-om, sp##k, f[kb]))));
+  const float g0 = fmaf(-om, f[0] - e0, f[0]);
+#define WT_OUT(k, kb)                                                   \
+  const float g##k = fmaf(-omm, sm##k, fmaf(-om, sp##k, f[k]));         \
+  const float g##kb = fmaf(omm, sm##k, fmaf(-om, sp##k, f[kb]));
   WT_OUT(1, 2) WT_OUT(3, 4) WT_OUT(5, 6) WT_OUT(7, 8) WT_OUT(9, 10) WT_OUT(11, 12) WT_OUT(13, 14)
   WT_OUT(15, 16) WT_OUT(17, 18)
 #undef WT_OUT
+  if constexpr (std::is_same<S, __half>::value) {
+    if (a.f16_sr) {
+      // stochastic rounding to half: each opposite pair is converted together
+      // with 32 random bits from a per-cell, per-step xorshift chain
+      uint32_t h = ((uint32_t)i ^ (uint32_t)(i >> 32)) * 0x9E3779B1u ^ a.sr_seed;
+      h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+      constexpr float SC = (float)WT_F16_SCALE;
+#define WT_SR(k, kb)                                                               \
+  {                                                                                \
+    h ^= h << 13; h ^= h >> 17; h ^= h << 5;                                       \
+    const __half2 p = sr_half2(g##k * SC, g##kb * SC, h);                          \
+    out.put(k, __high2half(p));                                                    \
+    out.put(kb, __low2half(p));                                                    \
+  }
+      WT_SR(1, 2) WT_SR(3, 4) WT_SR(5, 6) WT_SR(7, 8) WT_SR(9, 10) WT_SR(11, 12)
+      WT_SR(13, 14) WT_SR(15, 16) WT_SR(17, 18)
+#undef WT_SR
+      h ^= h << 13; h ^= h >> 17; h ^= h << 5;
+      out.put(0, __low2half(sr_half2(0.0f, g0 * SC, h)));
+      return;
+    }
+  }
+  out.put(0, Store<S>::from_f(g0));
+#define WT_PUT(k, kb) out.put(k, Store<S>::from_f(g##k)); out.put(kb, Store<S>::from_f(g##kb));
+  WT_PUT(1, 2) WT_PUT(3, 4) WT_PUT(5, 6) WT_PUT(7, 8) WT_PUT(9, 10) WT_PUT(11, 12) WT_PUT(13, 14)
+  WT_PUT(15, 16) WT_PUT(17, 18)
+#undef WT_PUT
 }
 
 // Float64 collision in the exact operation order of js/lbm.js:377-460. The

@@ -139,6 +139,7 @@ class LBM:
     side_bc = _param("side_bc", int)
     math = _param("math", int)
     kernel = _param("kernel", int)
+    f16_rounding = _param("f16_rounding", int)
     del _param
 
     @property
@@ -165,6 +166,8 @@ class LBM:
                 v = MATH[v]
             if key == "kernel" and isinstance(v, str):
                 v = KERNEL[v]
+            if key == "f16_rounding" and isinstance(v, str):
+                v = {"nearest": W.WT_ROUND_NEAREST, "stochastic": W.WT_ROUND_STOCHASTIC}[v]
             cur = getattr(self._p, key)
             setattr(self._p, key, float(v) if isinstance(cur, float) else int(v))
         try:
