@@ -192,6 +192,25 @@ int wt_get_body_stats(const wt_lattice* h, wt_body_stats* out);
  * density (the state is then left as computed). */
 int wt_step(wt_lattice* h, int nsteps, double* forces);
 
+/* wt_step without any device or pinned allocation. This entry point has no
+ * counterpart in the reference; it is for callers that cannot let the
+ * library allocate while they run: a host whose own memory pool owns the
+ * device, or code recording its work into a CUDA graph. wt_step may grow
+ * its force-series buffers; this call keeps the force partials, the
+ * per-step forces and the error word in one fixed device array of about
+ * 3.2 MB instead (16384 wall segments x 8 steps of partials, 4096 steps of
+ * forces), located once per device with cudaGetSymbolAddress.
+ * Same results as wt_step with the direct kernel (kernel AUTO or DIRECT).
+ * Limits: nsteps in 0..4096 (else WT_ERR_ARG); a body with more than 16384
+ * 32-cell wall segments gives WT_ERR_UNSUPPORTED; the lattice's device must
+ * be the current device (else WT_ERR_STATE). The first call on a device sets
+ * the scratch up and may load device code: make it (nsteps = 0 is enough)
+ * before any stream capture. The scratch is shared by every lattice on the
+ * device, so calls that overlap in time, from two threads or on two
+ * lattices, race and give wrong forces. forces (optional) receives
+ * 3*nsteps doubles as for wt_step. */
+int wt_step_noalloc(wt_lattice* h, int nsteps, double* forces);
+
 /* LBM.force — js/lbm.js:113, :289: the force of the last step. */
 int wt_get_force(const wt_lattice* h, double out[3]);
 

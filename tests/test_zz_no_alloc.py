@@ -1,0 +1,69 @@
+"""wt_step_noalloc: the step that allocates nothing, against wt_step.
+
+Two lattices get the same set-up; one advances with wt_step, the other with
+wt_step_noalloc, both called straight through the C ABI, twice in a row.
+The force series and the populations must agree (the two calls run the same
+kernels in the same order, so they agree exactly; the tolerance below is the
+fast-collision test tolerance). The file is named to be collected last, so
+that it also runs after every other test has used the device.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from lbm_cases import CFG0, apply_case, rel_linf
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-6
+
+
+def _lattice(storage, ground=False):
+    from windtunnel_b200.lbm import LBM
+    sim = LBM(CFG0["nx"], CFG0["ny"], CFG0["nz"], storage=storage)
+    apply_case(sim, u0=CFG0["u0"], tau=CFG0["tau"], csm=CFG0["csm"], lam=CFG0["lam"],
+               sphere=CFG0["sphere"], ground=ground, seed=CFG0["seed"], amp=CFG0["amp"])
+    return sim
+
+
+def _steps(fn, sim, n):
+    out = np.empty(3 * n, np.float64)
+    code = fn(sim._h, n, out.ctypes.data_as(C.POINTER(C.c_double)))
+    assert code == 0, _err(sim)
+    return out.reshape(n, 3)
+
+
+def _err(sim):
+    from windtunnel_b200 import _lib
+    return _lib.lib().wt_last_error(sim._h).decode()
+
+
+@pytest.mark.parametrize("storage,ground", [("f32", False), ("f32", True), ("f16dev", False),
+                                            ("f64", False)])
+def test_noalloc_matches_step_two_calls(wt_lib, storage, ground):
+    a = _lattice(storage, ground)
+    b = _lattice(storage, ground)
+    for n in (37, 20):              # two calls in a row, neither a multiple of the chunk
+        fa = _steps(wt_lib.wt_step, a, n)
+        fb = _steps(wt_lib.wt_step_noalloc, b, n)
+        assert np.abs(fa).max() > 0
+        assert rel_linf(fb, fa) <= TOL
+        assert rel_linf(b.populations("f"), a.populations("f")) <= TOL
+        assert b.steps == a.steps and b.parity == a.parity
+        assert b.force == pytest.approx(a.force, rel=TOL)
+    assert rel_linf(b.ux, a.ux) <= TOL
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch(wt_lib):
+    from windtunnel_b200 import _lib
+    sim = _lattice("f32")
+    assert wt_lib.wt_step_noalloc(sim._h, 4097, None) == _lib.WT_ERR_ARG
+    assert "0..4096" in _err(sim)
+    assert wt_lib.wt_step_noalloc(sim._h, -1, None) == _lib.WT_ERR_ARG
+    assert sim.steps == 0
+    assert wt_lib.wt_step_noalloc(sim._h, 0, None) == _lib.WT_OK
+    sim.set_params(kernel="staged")
+    assert wt_lib.wt_step_noalloc(sim._h, 1, None) == _lib.WT_ERR_UNSUPPORTED
+    assert "direct kernel" in _err(sim)
+    assert sim.steps == 0

@@ -119,6 +119,7 @@ SIGNATURES = {
                          _D, C.c_int, C.c_double],
     "wt_get_body_stats": [_P, C.POINTER(wt_body_stats)],
     "wt_step": [_P, C.c_int, _D],
+    "wt_step_noalloc": [_P, C.c_int, _D],
     "wt_get_force": [_P, _D],
     "wt_get_steps": [_P, C.POINTER(C.c_int64), _I],
     "wt_get_fields": [_P, _F, _F, _F, _F],

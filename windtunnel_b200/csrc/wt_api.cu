@@ -4,6 +4,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -826,3 +827,134 @@ int wt_get_launch_count(const wt_lattice* h, int64_t* count) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// wt_step_noalloc: the step for callers that must not allocate device memory
+// while they run, such as a host whose own memory pool owns the whole
+// device, or a caller that records the work into a CUDA graph, where an
+// allocation is not allowed. wt_step may grow its force series buffers
+// (cudaMalloc / cudaMallocHost); this entry point instead keeps the force
+// partials, the per-step forces and the error words in one fixed device
+// array declared below, found once per device with cudaGetSymbolAddress.
+namespace {
+
+constexpr int kNaSlots = 16384;     // force-partial slots (32-cell segments next to a wall)
+constexpr int kNaChunk = 8;         // steps whose partials are reduced together
+constexpr int kNaMaxSteps = 4096;   // steps per call
+constexpr int kNaMaxDevices = 64;
+constexpr size_t kNaPartBytes = sizeof(double) * 3 * (size_t)kNaSlots * kNaChunk;   // 3 MiB
+constexpr size_t kNaForceBytes = sizeof(double) * 3 * (size_t)kNaMaxSteps;          // 96 KiB
+constexpr size_t kNaErrOffset = kNaPartBytes + kNaForceBytes;
+constexpr size_t kNaBytes = kNaErrOffset + 256;   // error word, then 4 diagnostic words
+
+// The scratch: partials | forces | error word (4 B, 8 B pad) | diagnostics (32 B).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+std::mutex g_na_mu;
+unsigned char* g_na_ptr[kNaMaxDevices] = {};
+
+// Device address of the scratch on `dev`, which must be the current device.
+// The first call on a device may load the module's device code, so it must
+// not happen while a stream is being captured.
+int noalloc_scratch(wt_lattice* h, int dev, unsigned char** out) {
+  if (dev < 0 || dev >= kNaMaxDevices) return fail(h, WT_ERR_UNSUPPORTED, "device index too large");
+  std::lock_guard<std::mutex> lock(g_na_mu);
+  if (!g_na_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGetSymbolAddress(noalloc scratch)");
+    g_na_ptr[dev] = (unsigned char*)p;
+  }
+  *out = g_na_ptr[dev];
+  return WT_OK;
+}
+
+template <class S, class L>
+void run_steps_noalloc(wt_lattice* h, int nsteps, L launch, double* part, double* forces,
+                       unsigned* err, long long* diag) {
+  wt::StepArgs<S> a = make_args<S>(h);
+  a.err = err;
+  a.diag = diag;
+  const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
+  const bool wide = 19 * h->n >= (1LL << 31);
+  const size_t stride = 3 * (size_t)h->nslots;
+  for (int done = 0; done < nsteps;) {
+    const int chunk = std::min(kNaChunk, nsteps - done);
+    for (int s = 0; s < chunk; s++) {
+      a.F = (const S*)h->buf[h->parity];
+      a.G = (S*)h->buf[h->parity ^ 1];
+      a.part = part + (size_t)s * stride;
+      a.write_fields = (done + s == nsteps - 1) ? 1 : 0;
+      a.sr_seed = (unsigned)((uint64_t)(h->steps + done + s) * 0x9E3779B97F4A7C15ULL >> 32);
+      launch(a, grid, wide, h->stream);
+      h->launches++;
+      h->parity ^= 1;
+    }
+    wt::launch_force_reduce(part, (unsigned)h->nslots, chunk, forces + 3 * (size_t)done,
+                            h->stream);
+    h->launches++;
+    done += chunk;
+  }
+}
+
+}  // namespace
+
+extern "C" int wt_step_noalloc(wt_lattice* h, int nsteps, double* forces) {
+  if (!h) return WT_ERR_ARG;
+  if (nsteps < 0 || nsteps > kNaMaxSteps)
+    return fail(h, WT_ERR_ARG, "wt_step_noalloc: nsteps must be in 0.." +
+                                   std::to_string(kNaMaxSteps));
+  if (h->nslots > kNaSlots)
+    return fail(h, WT_ERR_UNSUPPORTED,
+                "wt_step_noalloc: the body has " + std::to_string(h->nslots) +
+                    " wall segments, more than the " + std::to_string(kNaSlots) +
+                    " its fixed scratch holds; use wt_step");
+  if (h->p.kernel != WT_KERNEL_AUTO && h->p.kernel != WT_KERNEL_DIRECT)
+    return fail(h, WT_ERR_UNSUPPORTED, "wt_step_noalloc runs the direct kernel only");
+  int dev = -1;
+  WT_CUDA(h, cudaGetDevice(&dev));
+  if (dev != h->device)
+    return fail(h, WT_ERR_STATE, "wt_step_noalloc: make the lattice's device current first");
+  unsigned char* base = nullptr;
+  int c = noalloc_scratch(h, dev, &base);
+  if (c != WT_OK) return c;
+  if (nsteps == 0) return WT_OK;
+  double* part = (double*)base;
+  double* fdev = (double*)(base + kNaPartBytes);
+  unsigned* err = (unsigned*)(base + kNaErrOffset);
+  long long* diag = (long long*)(base + kNaErrOffset + 8);
+  // Only the error and diagnostic words must start at zero: every used
+  // partial slot and every force entry is written before it is read.
+  WT_CUDA(h, cudaMemsetAsync(err, 0, 8 + 4 * sizeof(long long), h->stream));
+  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
+  switch (h->storage) {
+    case WT_STORE_F32:
+      if (exact) run_steps_noalloc<float>(h, nsteps, wt::launch_step_f32_exact, part, fdev, err, diag);
+      else run_steps_noalloc<float>(h, nsteps, wt::launch_step_f32_fast, part, fdev, err, diag);
+      break;
+    case WT_STORE_F16DEV:
+      run_steps_noalloc<__half>(h, nsteps, wt::launch_step_f16_fast, part, fdev, err, diag);
+      break;
+    default:
+      run_steps_noalloc<double>(h, nsteps, wt::launch_step_f64_exact, part, fdev, err, diag);
+      break;
+  }
+  WT_CUDA(h, cudaGetLastError());
+  double last[3] = {0, 0, 0};
+  unsigned errw = 0;
+  if (forces)
+    WT_CUDA(h, cudaMemcpyAsync(forces, fdev, sizeof(double) * 3 * (size_t)nsteps,
+                               cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaMemcpyAsync(last, fdev + 3 * (size_t)(nsteps - 1), sizeof(last),
+                             cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaMemcpyAsync(&errw, err, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->steps += nsteps;
+  h->force[0] = last[0]; h->force[1] = last[1]; h->force[2] = last[2];
+  if (errw & 2u)
+    return fail(h, WT_ERR_STATE, "a near-wall warp had no force slot (occupancy changed "
+                                 "without voxelize)");
+  if (errw & 1u)
+    return fail(h, WT_ERR_DIVERGED, "a step produced a non-finite or non-positive density");
+  return WT_OK;
+}
