@@ -194,8 +194,10 @@ int wt_step(wt_lattice* h, int nsteps, double* forces);
 
 /* wt_step without any device or pinned allocation. This entry point has no
  * counterpart in the reference; it is for callers that cannot let the
- * library allocate while they run: a host whose own memory pool owns the
- * device, or code recording its work into a CUDA graph. wt_step may grow
+ * library allocate while they run: a host whose own memory pool has already
+ * claimed the device's memory (so a cudaMalloc would fail), or a host
+ * stepping inside a frame loop that must not stall, since cudaMalloc and
+ * cudaFree may synchronise the whole device. wt_step may grow
  * its force-series buffers; this call keeps the force partials, the
  * per-step forces and the error word in one fixed device array of about
  * 3.2 MB instead (16384 wall segments x 8 steps of partials, 4096 steps of

@@ -830,9 +830,10 @@ int wt_get_launch_count(const wt_lattice* h, int64_t* count) {
 
 // ---------------------------------------------------------------------------
 // wt_step_noalloc: the step for callers that must not allocate device memory
-// while they run, such as a host whose own memory pool owns the whole
-// device, or a caller that records the work into a CUDA graph, where an
-// allocation is not allowed. wt_step may grow its force series buffers
+// while they run, such as a host whose own memory pool has already claimed
+// the device's memory, or a host stepping inside a frame loop that must not
+// stall (cudaMalloc / cudaFree may synchronise the whole device). wt_step
+// may grow its force series buffers
 // (cudaMalloc / cudaMallocHost); this entry point instead keeps the force
 // partials, the per-step forces and the error words in one fixed device
 // array declared below, found once per device with cudaGetSymbolAddress.
