@@ -78,8 +78,15 @@ enum {
                             needs nx to be a multiple of 16 bytes / element size */
   WT_KERNEL_VECTOR = 3,  /* two cells per thread, paired vector loads and stores with warp
                             shuffles for the x-shifted directions; float32 collision, nx even */
-  WT_KERNEL_PIPE = 4     /* one thread per cell for 8 z planes, the next cell's loads issued
+  WT_KERNEL_PIPE = 4,    /* one thread per cell for 8 z planes, the next cell's loads issued
                             before the current cell's collision; float32 collision */
+  WT_KERNEL_X2 = 5,      /* two cells per thread with paired vector loads / stores and the
+                            collision of both cells in packed float32x2 instructions; float32
+                            collision, nx even, nearest rounding for half storage */
+  WT_KERNEL_TMA = 6      /* persistent CTAs moving 128x4-cell tiles of all 19 directions through
+                            shared memory with tensor-map TMA loads and stores, packed float32x2
+                            collision; float32 collision, nx a multiple of 16 bytes / element,
+                            nearest rounding for half storage */
 };
 
 /* Rounding of half-precision stores. Stochastic rounding draws its random
@@ -105,7 +112,7 @@ typedef struct wt_params {
   int32_t side_bc;   /* WT_SIDE_EQ (default) or WT_SIDE_FREESLIP */
   int32_t math;      /* WT_MATH_FAST (default) or WT_MATH_EXACT */
   int32_t kernel;    /* WT_KERNEL_* (default WT_KERNEL_AUTO) */
-  int32_t f16_rounding; /* half storage: WT_ROUND_NEAREST or WT_ROUND_STOCHASTIC (default) */
+  int32_t f16_rounding; /* half storage: WT_ROUND_NEAREST (default) or WT_ROUND_STOCHASTIC */
   int32_t reserved;  /* must be 0 */
 } wt_params;
 
@@ -212,6 +219,42 @@ int wt_step(wt_lattice* h, int nsteps, double* forces);
  * lattices, race and give wrong forces. forces (optional) receives
  * 3*nsteps doubles as for wt_step. */
 int wt_step_noalloc(wt_lattice* h, int nsteps, double* forces);
+
+/* Partial bounce-back field (no reference counterpart; the differentiable
+ * body of the adjoint): solid fraction s in [0, 1] for every cell of the
+ * half-open box {x0, y0, z0, x1, y1, z1}, x fastest. A fluid cell with
+ * fraction s stores g_q = (1 - s) gc_q + s f_opp(q) (gc collided, f pulled)
+ * and adds s * sum_q c_q (gc_q - f_opp(q)) to the force. box == NULL clears
+ * the field. While a field is set the step runs the direct kernel. */
+int wt_set_solid_fraction(wt_lattice* h, const int box[6], const double* s);
+
+/* Objective and checkpointing of wt_adjoint. */
+typedef struct wt_adj_cfg {
+  int32_t nsteps;      /* forward steps from the current state */
+  int32_t window;      /* J = mean of the force component over the last `window` steps */
+  int32_t component;   /* 0 = x (drag), 1 = y, 2 = z */
+  int32_t checkpoint;  /* steps between stored states; 0 = ceil(sqrt(nsteps)) */
+  int32_t reserved[4]; /* must be 0 */
+} wt_adj_cfg;
+
+typedef struct wt_adj_stats {
+  double J;            /* the objective */
+  double forward_ms;   /* forward sweep with checkpoint copies (CUDA events) */
+  double backward_ms;  /* recomputation + adjoint steps (CUDA events) */
+  int64_t device_bytes;/* device memory the run allocated (checkpoints, segment, adjoint) */
+  int32_t checkpoints; /* stored states */
+  int32_t segment;     /* steps per checkpoint interval */
+} wt_adj_stats;
+
+/* d(J)/d(s) by the discrete adjoint of the step (no reference counterpart).
+ * Runs cfg->nsteps steps from the current state (the lattice ends where
+ * wt_step(h, nsteps) would leave it) storing a checkpoint every
+ * cfg->checkpoint steps, then runs the adjoint backwards, recomputing each
+ * interval's states from its checkpoint. dJds receives one double per cell
+ * of the solid-fraction box (x fastest). Adjoint arithmetic: float64 for
+ * float64 storage or WT_MATH_EXACT, float32 otherwise. Stationary walls only
+ * (WT_ERR_UNSUPPORTED with moving walls); WT_ERR_STATE without a field. */
+int wt_adjoint(wt_lattice* h, const wt_adj_cfg* cfg, double* dJds, wt_adj_stats* stats);
 
 /* LBM.force — js/lbm.js:113, :289: the force of the last step. */
 int wt_get_force(const wt_lattice* h, double out[3]);

@@ -137,6 +137,155 @@ static int or_cmp_int(const void* a, const void* b) {
   return (x > y) - (x < y);
 }
 
+/* ---- partial bounce-back and its discrete adjoint (no reference counterpart) ----
+ *
+ * Forward, per computed fluid cell with solid fraction s:
+ *   g_q = (1 - s) gc_q + s f_opp(q),  F += s sum_q c_q (gc_q - f_opp(q)),
+ * gc the collided populations and f the pulled ones. The objective is
+ * J = mean over the last `window` steps of force component `comp`.
+ *
+ * The adjoint runs backwards in time over the stored forward states. T^t[q][i]
+ * holds dJ/d(pulled value of link q at cell i, step t); the adjoint of the
+ * population stored at location (q, j) after step t is the sum of T^{t+1} over
+ * the links that pull it at step t+1 (or_adj_gather below), so every adjoint
+ * step is a pull like the forward step. Quantities of the forward collision
+ * are recomputed per cell from the stored pre-step state, in the operation
+ * order of js/lbm.js:377-460. */
+typedef struct {
+  double f[OR_Q], gc[OR_Q], n[OR_Q];
+  double dr, r, inv, jx, jy, jz, vx, vy, vz, usq, A, r3, r45;
+  double pxx, pyy, pzz, pxy, pxz, pyz, mag, R, tauEff, om, omm;
+} or_cellfw;
+
+/* Forward collision of one cell from its pulled populations f (already in
+ * c->f), js/lbm.js:377-460, keeping the intermediates. */
+static void or_collide_fw(const wt_params* p, or_cellfw* c) {
+  const double* f = c->f;
+  const double W0 = 1.0 / 3, WF = 1.0 / 18, WE = 1.0 / 36;
+  const double dr = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] +
+                    f[11] + f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
+  const double r = 1 + dr;
+  const double inv = 1 / r;
+  const double jx = f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[11] - f[12] + f[13] - f[14];
+  const double jy = f[3] - f[4] + f[7] - f[8] - f[9] + f[10] + f[15] - f[16] + f[17] - f[18];
+  const double jz = f[5] - f[6] + f[11] - f[12] - f[13] + f[14] + f[15] - f[16] - f[17] + f[18];
+  const double vx = jx * inv, vy = jy * inv, vz = jz * inv;
+  const double usq = vx * vx + vy * vy + vz * vz;
+  const double A = dr - r * 1.5 * usq;
+  const double r3 = 3 * r, r45 = 4.5 * r;
+  double e[OR_Q];
+  e[0] = W0 * A;
+  for (int q = 1; q < OR_Q; q++) {
+    const double cv = OR_EX[q] * vx + OR_EY[q] * vy + OR_EZ[q] * vz;
+    e[q] = OR_W[q] * (A + r3 * cv + r45 * cv * cv);
+  }
+  (void)WF; (void)WE;
+  for (int q = 0; q < OR_Q; q++) c->n[q] = f[q] - e[q];
+  const double* n = c->n;
+  const double tau0 = p->tau;
+  double om = 1 / tau0, tauEff = tau0;
+  c->pxx = c->pyy = c->pzz = c->pxy = c->pxz = c->pyz = c->mag = c->R = 0;
+  if (p->les) {
+    c->pxx = n[1] + n[2] + n[7] + n[8] + n[9] + n[10] + n[11] + n[12] + n[13] + n[14];
+    c->pyy = n[3] + n[4] + n[7] + n[8] + n[9] + n[10] + n[15] + n[16] + n[17] + n[18];
+    c->pzz = n[5] + n[6] + n[11] + n[12] + n[13] + n[14] + n[15] + n[16] + n[17] + n[18];
+    c->pxy = n[7] + n[8] - n[9] - n[10];
+    c->pxz = n[11] + n[12] - n[13] - n[14];
+    c->pyz = n[15] + n[16] - n[17] - n[18];
+    c->mag = sqrt(2 * (c->pxx * c->pxx + c->pyy * c->pyy + c->pzz * c->pzz +
+                       2 * (c->pxy * c->pxy + c->pxz * c->pxz + c->pyz * c->pyz)));
+    const double SQ18 = 18 * OR_SQRT2;
+    c->R = sqrt(tau0 * tau0 + SQ18 * (p->csm * p->csm) * c->mag * inv);
+    tauEff = 0.5 * (tau0 + c->R);
+    om = 1 / tauEff;
+  }
+  const double omm = p->trt ? 1 / (0.5 + p->lambda / (tauEff - 0.5)) : om;
+  c->gc[0] = f[0] - om * (f[0] - e[0]);
+  for (int a = 1; a < OR_Q; a += 2) {
+    const double sp = 0.5 * (n[a] + n[a + 1]), sm = 0.5 * (n[a] - n[a + 1]);
+    c->gc[a] = f[a] - om * sp - omm * sm;
+    c->gc[a + 1] = f[a + 1] - om * sp + omm * sm;
+  }
+  c->dr = dr; c->r = r; c->inv = inv; c->jx = jx; c->jy = jy; c->jz = jz;
+  c->vx = vx; c->vy = vy; c->vz = vz; c->usq = usq; c->A = A; c->r3 = r3; c->r45 = r45;
+  c->tauEff = tauEff; c->om = om; c->omm = omm;
+}
+
+/* Vector-Jacobian product of or_collide_fw: fb += (d gc / d f)^T a. */
+static void or_collide_vjp(const wt_params* p, const or_cellfw* c, const double a[OR_Q],
+                           double fb[OR_Q]) {
+  const double* n = c->n;
+  double nb[OR_Q];
+  for (int q = 0; q < OR_Q; q++) fb[q] += a[q];
+  double omb = -(a[0] * n[0]);
+  double ommb = 0;
+  nb[0] = -(c->om * a[0]);
+  for (int k = 1; k < OR_Q; k += 2) {
+    const double sp = 0.5 * (n[k] + n[k + 1]), sm = 0.5 * (n[k] - n[k + 1]);
+    const double as = a[k] + a[k + 1], ad = a[k] - a[k + 1];
+    omb -= as * sp;
+    ommb -= ad * sm;
+    const double spb = -(c->om * as), smb = -(c->omm * ad);
+    nb[k] = 0.5 * (spb + smb);
+    nb[k + 1] = 0.5 * (spb - smb);
+  }
+  double invb = 0;
+  if (p->les) {
+    double teb;
+    if (p->trt) {
+      const double tm = c->tauEff - 0.5;
+      teb = ommb * (c->omm * c->omm * p->lambda / (tm * tm)) - omb * (c->om * c->om);
+    } else {
+      teb = -(omb + ommb) * (c->om * c->om);
+    }
+    const double Rb = 0.5 * teb;
+    const double Xb = Rb / (2 * c->R);
+    const double K = 18 * OR_SQRT2 * (p->csm * p->csm);
+    const double magb = Xb * K * c->inv;
+    invb += Xb * K * c->mag;
+    const double Qb = c->mag > 0 ? magb / c->mag : 0;
+    const double pxxb = 2 * c->pxx * Qb, pyyb = 2 * c->pyy * Qb, pzzb = 2 * c->pzz * Qb;
+    const double pxyb = 4 * c->pxy * Qb, pxzb = 4 * c->pxz * Qb, pyzb = 4 * c->pyz * Qb;
+    nb[1] += pxxb; nb[2] += pxxb;
+    nb[3] += pyyb; nb[4] += pyyb;
+    nb[5] += pzzb; nb[6] += pzzb;
+    nb[7] += pxxb + pyyb + pxyb; nb[8] += pxxb + pyyb + pxyb;
+    nb[9] += pxxb + pyyb - pxyb; nb[10] += pxxb + pyyb - pxyb;
+    nb[11] += pxxb + pzzb + pxzb; nb[12] += pxxb + pzzb + pxzb;
+    nb[13] += pxxb + pzzb - pxzb; nb[14] += pxxb + pzzb - pxzb;
+    nb[15] += pyyb + pzzb + pyzb; nb[16] += pyyb + pzzb + pyzb;
+    nb[17] += pyyb + pzzb - pyzb; nb[18] += pyyb + pzzb - pyzb;
+  }
+  /* n = f - e */
+  double Ab = 0, r3b = 0, r45b = 0, vxb = 0, vyb = 0, vzb = 0;
+  for (int q = 0; q < OR_Q; q++) {
+    fb[q] += nb[q];
+    const double eb = -nb[q];
+    Ab += OR_W[q] * eb;
+    if (q > 0) {
+      const double cv = OR_EX[q] * c->vx + OR_EY[q] * c->vy + OR_EZ[q] * c->vz;
+      const double web = OR_W[q] * eb;
+      r3b += web * cv;
+      r45b += web * (cv * cv);
+      const double cvb = web * (c->r3 + 2 * c->r45 * cv);
+      vxb += OR_EX[q] * cvb; vyb += OR_EY[q] * cvb; vzb += OR_EZ[q] * cvb;
+    }
+  }
+  /* A = dr - r * 1.5 * usq */
+  double drb = Ab;
+  double rb = 3 * r3b + 4.5 * r45b - 1.5 * c->usq * Ab;
+  const double usqb = -(c->r * 1.5 * Ab);
+  vxb += 2 * c->vx * usqb; vyb += 2 * c->vy * usqb; vzb += 2 * c->vz * usqb;
+  /* v = j * inv */
+  invb += vxb * c->jx + vyb * c->jy + vzb * c->jz;
+  const double jxb = vxb * c->inv, jyb = vyb * c->inv, jzb = vzb * c->inv;
+  /* inv = 1 / r, r = 1 + dr */
+  rb -= c->inv * c->inv * invb;
+  drb += rb;
+  for (int q = 0; q < OR_Q; q++)
+    fb[q] += drb + (OR_EX[q] * jxb + OR_EY[q] * jyb + OR_EZ[q] * jzb);
+}
+
 #define OR_CAT2(a, b) a##b
 #define OR_CAT(a, b) OR_CAT2(a, b)
 

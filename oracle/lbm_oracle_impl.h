@@ -27,6 +27,9 @@ typedef struct {
   double force[3];
   int frontal, planform, solid_cells, ride_height, ground;
   long steps;
+  /* partial bounce-back: solid fraction on the half-open box sbox (x0,y0,z0,x1,y1,z1) */
+  double* sfrac;
+  int sbox[6];
 } OR_FN(lbm);
 
 void OR_FN(destroy)(OR_FN(lbm) * L);
@@ -129,6 +132,7 @@ void OR_FN(destroy)(OR_FN(lbm) * L) {
   free(L->bufA); free(L->bufB); free(L->solid); free(L->near_);
   free(L->ux); free(L->uy); free(L->uz); free(L->rho);
   free(L->uwx); free(L->uwy); free(L->uwz);
+  free(L->sfrac);
   free(L);
 }
 
@@ -240,6 +244,31 @@ int OR_FN(voxelize_mask)(OR_FN(lbm) * L, const double box[6], const uint8_t* ins
   L->ride_height = ng ? gaps[ng >> 1] : 0;
   free(gaps); free(col); free(plan); free(low);
   OR_FN(rebuild_near)(L);
+  return 0;
+}
+
+/* Solid fraction of cell (x,y,z): 0 outside the partial bounce-back box. */
+static inline double OR_FN(sfrac_at)(const OR_FN(lbm) * L, int x, int y, int z) {
+  if (!L->sfrac) return 0;
+  const int* b = L->sbox;
+  if (x < b[0] || x >= b[3] || y < b[1] || y >= b[4] || z < b[2] || z >= b[5]) return 0;
+  return L->sfrac[(x - b[0]) + (long)(b[3] - b[0]) * ((y - b[1]) + (long)(b[4] - b[1]) * (z - b[2]))];
+}
+
+/* Set the partial bounce-back field: s holds one value per cell of the
+ * half-open box, x fastest; box == NULL clears it. */
+int OR_FN(set_solid_fraction)(OR_FN(lbm) * L, const int box[6], const double* sv) {
+  free(L->sfrac);
+  L->sfrac = NULL;
+  if (!box) return 0;
+  const long m = (long)(box[3] - box[0]) * (box[4] - box[1]) * (box[5] - box[2]);
+  if (box[0] < 0 || box[1] < 0 || box[2] < 0 || box[3] > L->nx || box[4] > L->ny ||
+      box[5] > L->nz || m <= 0)
+    return -1;
+  L->sfrac = (double*)malloc(sizeof(double) * (size_t)m);
+  if (!L->sfrac) return -2;
+  memcpy(L->sfrac, sv, sizeof(double) * (size_t)m);
+  memcpy(L->sbox, box, sizeof(int) * 6);
   return 0;
 }
 
@@ -382,27 +411,44 @@ static void OR_FN(step_slab)(OR_FN(lbm) * L, int z0, int z1, double sf[3]) {
         const double omm = trt ? 1 / (0.5 + lam / (tauEff - 0.5)) : om;
 
         /* collision in opposite pairs, js/lbm.js:440-460 */
-        const long ii = i;
-        G[0 * nn + ii] = (OR_T)(f0 - om * (f0 - e0));
+        double gc[OR_Q];
+        gc[0] = f0 - om * (f0 - e0);
         double sp, sm;
         sp = 0.5 * (n1 + n2); sm = 0.5 * (n1 - n2);
-        G[1 * nn + ii] = (OR_T)(f1 - om * sp - omm * sm); G[2 * nn + ii] = (OR_T)(f2 - om * sp + omm * sm);
+        gc[1] = f1 - om * sp - omm * sm; gc[2] = f2 - om * sp + omm * sm;
         sp = 0.5 * (n3 + n4); sm = 0.5 * (n3 - n4);
-        G[3 * nn + ii] = (OR_T)(f3 - om * sp - omm * sm); G[4 * nn + ii] = (OR_T)(f4 - om * sp + omm * sm);
+        gc[3] = f3 - om * sp - omm * sm; gc[4] = f4 - om * sp + omm * sm;
         sp = 0.5 * (n5 + n6); sm = 0.5 * (n5 - n6);
-        G[5 * nn + ii] = (OR_T)(f5 - om * sp - omm * sm); G[6 * nn + ii] = (OR_T)(f6 - om * sp + omm * sm);
+        gc[5] = f5 - om * sp - omm * sm; gc[6] = f6 - om * sp + omm * sm;
         sp = 0.5 * (n7 + n8); sm = 0.5 * (n7 - n8);
-        G[7 * nn + ii] = (OR_T)(f7 - om * sp - omm * sm); G[8 * nn + ii] = (OR_T)(f8 - om * sp + omm * sm);
+        gc[7] = f7 - om * sp - omm * sm; gc[8] = f8 - om * sp + omm * sm;
         sp = 0.5 * (n9 + n10); sm = 0.5 * (n9 - n10);
-        G[9 * nn + ii] = (OR_T)(f9 - om * sp - omm * sm); G[10 * nn + ii] = (OR_T)(f10 - om * sp + omm * sm);
+        gc[9] = f9 - om * sp - omm * sm; gc[10] = f10 - om * sp + omm * sm;
         sp = 0.5 * (n11 + n12); sm = 0.5 * (n11 - n12);
-        G[11 * nn + ii] = (OR_T)(f11 - om * sp - omm * sm); G[12 * nn + ii] = (OR_T)(f12 - om * sp + omm * sm);
+        gc[11] = f11 - om * sp - omm * sm; gc[12] = f12 - om * sp + omm * sm;
         sp = 0.5 * (n13 + n14); sm = 0.5 * (n13 - n14);
-        G[13 * nn + ii] = (OR_T)(f13 - om * sp - omm * sm); G[14 * nn + ii] = (OR_T)(f14 - om * sp + omm * sm);
+        gc[13] = f13 - om * sp - omm * sm; gc[14] = f14 - om * sp + omm * sm;
         sp = 0.5 * (n15 + n16); sm = 0.5 * (n15 - n16);
-        G[15 * nn + ii] = (OR_T)(f15 - om * sp - omm * sm); G[16 * nn + ii] = (OR_T)(f16 - om * sp + omm * sm);
+        gc[15] = f15 - om * sp - omm * sm; gc[16] = f16 - om * sp + omm * sm;
         sp = 0.5 * (n17 + n18); sm = 0.5 * (n17 - n18);
-        G[17 * nn + ii] = (OR_T)(f17 - om * sp - omm * sm); G[18 * nn + ii] = (OR_T)(f18 - om * sp + omm * sm);
+        gc[17] = f17 - om * sp - omm * sm; gc[18] = f18 - om * sp + omm * sm;
+        const double sfr = OR_FN(sfrac_at)(L, x, y, z);
+        if (sfr != 0) {
+          /* partial bounce-back (no reference counterpart): g = (1-s) gc + s f_opp,
+           * force += s * sum_q c_q (gc_q - f_opp(q)) */
+          const double fl[OR_Q] = {f0, f1, f2, f3, f4, f5, f6, f7, f8, f9,
+                                   f10, f11, f12, f13, f14, f15, f16, f17, f18};
+          double px = 0, py = 0, pz = 0;
+          for (int q = 0; q < OR_Q; q++) {
+            const double fo = fl[OR_OPP[q]];
+            const double d = gc[q] - fo;
+            px += OR_EX[q] * d; py += OR_EY[q] * d; pz += OR_EZ[q] * d;
+            G[q * nn + i] = (OR_T)((1 - sfr) * gc[q] + sfr * fo);
+          }
+          Fx += sfr * px; Fy += sfr * py; Fz += sfr * pz;
+        } else {
+          for (int q = 0; q < OR_Q; q++) G[q * nn + i] = (OR_T)gc[q];
+        }
       }
     }
   }
@@ -602,6 +648,158 @@ int OR_FN(is_solid)(OR_FN(lbm) * L, double x, double y, double z) {
   const int xi = or_toint32(x), yi = or_toint32(y), zi = or_toint32(z);
   if (xi < 0 || yi < 0 || zi < 0 || xi >= L->nx || yi >= L->ny || zi >= L->nz) return 0;
   return L->solid[xi + (long)L->nx * (yi + (long)L->ny * zi)] != 0;
+}
+
+
+/* ---- partial bounce-back adjoint (no reference counterpart) ---------------- */
+
+static inline int OR_FN(computed)(const OR_FN(lbm) * L, int x, int y, int z) {
+  return x >= 1 && x <= L->nx - 2 && y >= 1 && y <= L->ny - 2 && z >= 1 && z <= L->nz - 2 &&
+         !L->solid[x + (long)L->nx * (y + (long)L->ny * z)];
+}
+
+/* Pulled populations of computed cell (x,y,z) from state F, with the
+ * bounce-back and free-slip rules of step_slab (stationary walls). Sets bit q
+ * of *obj for every link q that bounces off the body (SOLID_OBJ). */
+static void OR_FN(adj_pull)(OR_FN(lbm) * L, const OR_T* F, int x, int y, int z, double f[OR_Q],
+                            unsigned* obj) {
+  const long nn = L->n;
+  const long i = x + (long)L->nx * (y + (long)L->ny * z);
+  const int shell = L->p.side_bc == 1 &&
+                    (y == 1 || y == L->ny - 2 || z == 1 || z == L->nz - 2);
+  *obj = 0;
+  for (int q = 0; q < OR_Q; q++) {
+    const long j = i - L->off[q];
+    const uint8_t s = L->solid[j];
+    if (s) {
+      f[q] = (double)F[(long)OR_OPP[q] * nn + i];
+      if (s == OR_SOLID_OBJ) *obj |= 1u << q;
+    } else if (shell) {
+      f[q] = OR_FN(gather_fs)(L, F, q, x, y, z);
+    } else {
+      f[q] = (double)F[L->src[q] + i];
+    }
+  }
+}
+
+/* Adjoint of the population stored at (q, location (x,y,z)) after a step:
+ * the sum of Tn over the links that pull it in the next step -- the plain
+ * consumer (x,y,z)+c_q, the location's own cell when that neighbour is solid
+ * (bounce-back), and the mirrored consumer when that neighbour is a free-slip
+ * side plane. Tn rows of cells that are not computed hold zeros. */
+static double OR_FN(adj_gather)(const OR_FN(lbm) * L, const double* Tn, int q, int x, int y, int z,
+                                int loc_computed) {
+  const int nx = L->nx, ny = L->ny, nz = L->nz;
+  const long nn = L->n;
+  const int px = x + OR_EX[q], py = y + OR_EY[q], pz = z + OR_EZ[q];
+  double v = 0;
+  if (px >= 0 && px < nx) v = Tn[(long)q * nn + px + (long)nx * (py + (long)ny * pz)];
+  if (loc_computed && L->solid[px + (long)nx * (py + (long)ny * pz)])
+    v += Tn[(long)OR_OPP[q] * nn + x + (long)nx * (y + (long)ny * z)];
+  if (L->p.side_bc == 1) {
+    const int ym = py == 0 || py == ny - 1, zm = pz == 0 || pz == nz - 1;
+    if (ym || zm) {
+      const int sy = ym ? py : y, sz = zm ? pz : z;
+      if (!L->solid[x + (long)nx * (sy + (long)ny * sz)] && px >= 0 && px < nx) {
+        const int cy = ym ? y : py, cz = zm ? z : pz;
+        int qq = q;
+        if (ym) qq = OR_MY[qq];
+        if (zm) qq = OR_MZ[qq];
+        v += Tn[(long)qq * nn + px + (long)nx * (cy + (long)ny * cz)];
+      }
+    }
+  }
+  return v;
+}
+
+/* One adjoint step: Tc from Tn over the pre-step state F, with force weight
+ * wJ on component comp; accumulates dJ/ds into ds (box cells). */
+static void OR_FN(adj_step)(OR_FN(lbm) * L, const OR_T* F, const double* Tn, double* Tc, double wJ,
+                            int comp, double* ds) {
+  const int nx = L->nx, ny = L->ny, nz = L->nz;
+  const long nn = L->n;
+  const int* CC = comp == 0 ? OR_EX : (comp == 1 ? OR_EY : OR_EZ);
+  for (int z = 0; z < nz; z++) {
+    for (int y = 0; y < ny; y++) {
+      for (int x = 0; x < nx; x++) {
+        const long i = x + (long)nx * (y + (long)ny * z);
+        if (!OR_FN(computed)(L, x, y, z)) {
+          for (int q = 0; q < OR_Q; q++) Tc[q * nn + i] = 0;
+          continue;
+        }
+        double gb[OR_Q];
+        for (int q = 0; q < OR_Q; q++) {
+          gb[q] = OR_FN(adj_gather)(L, Tn, q, x, y, z, 1);
+          if (x == nx - 2) gb[q] += OR_FN(adj_gather)(L, Tn, q, x + 1, y, z, 0);  /* outlet copy */
+        }
+        or_cellfw c;
+        unsigned obj;
+        OR_FN(adj_pull)(L, F, x, y, z, c.f, &obj);
+        or_collide_fw(&L->p, &c);
+        const double s = OR_FN(sfrac_at)(L, x, y, z);
+        double a[OR_Q], fb[OR_Q];
+        for (int q = 0; q < OR_Q; q++) {
+          a[q] = (1 - s) * gb[q] + wJ * s * CC[q];
+          fb[q] = s * gb[OR_OPP[q]] + wJ * s * CC[q];
+          if ((obj >> q) & 1u) fb[q] -= 2 * wJ * CC[q];
+        }
+        if (L->sfrac) {
+          const int* b = L->sbox;
+          if (x >= b[0] && x < b[3] && y >= b[1] && y < b[4] && z >= b[2] && z < b[5]) {
+            /* dJ/ds = sum_q gb_q (f_opp(q) - gc_q) + wJ sum_q c_q (gc_q - f_opp(q)) */
+            double g1 = 0, g2 = 0;
+            for (int q = 0; q < OR_Q; q++) {
+              const double d = c.f[OR_OPP[q]] - c.gc[q];
+              g1 += gb[q] * d;
+              g2 -= CC[q] * d;
+            }
+            ds[(x - b[0]) + (long)(b[3] - b[0]) * ((y - b[1]) + (long)(b[4] - b[1]) * (z - b[2]))] +=
+                g1 + wJ * g2;
+          }
+        }
+        or_collide_vjp(&L->p, &c, a, fb);
+        for (int q = 0; q < OR_Q; q++) Tc[q * nn + i] = fb[q];
+      }
+    }
+  }
+}
+
+/* J = mean of force component comp over the last `window` of nsteps steps
+ * from the current state, and dJ/ds on the solid-fraction box (dJds, box
+ * cells, x fastest). Runs the forward (the lattice ends nsteps later, as
+ * after step()) keeping every state, then the adjoint backwards. Stationary
+ * walls only. Returns 0, or <0 on bad arguments / allocation failure. */
+int OR_FN(adjoint)(OR_FN(lbm) * L, int nsteps, int window, int comp, double* J, double* dJds) {
+  if (nsteps < 1 || window < 1 || window > nsteps || comp < 0 || comp > 2 || !L->sfrac) return -1;
+  if (L->p.moving_walls) return -1;
+  const long nn = L->n;
+  const size_t pop = (size_t)nn * OR_Q;
+  OR_T* states = (OR_T*)malloc(sizeof(OR_T) * pop * (size_t)nsteps);
+  double* forces = (double*)malloc(sizeof(double) * 3 * (size_t)nsteps);
+  double* Tn = (double*)calloc(pop, sizeof(double));
+  double* Tc = (double*)calloc(pop, sizeof(double));
+  if (!states || !forces || !Tn || !Tc) {
+    free(states); free(forces); free(Tn); free(Tc);
+    return -2;
+  }
+  for (int t = 0; t < nsteps; t++) {
+    memcpy(states + pop * (size_t)t, OR_FN(cur_f)(L), sizeof(OR_T) * pop);
+    OR_FN(step)(L, 1, forces + 3 * (size_t)t, 1);
+  }
+  double acc = 0;
+  for (int t = nsteps - window; t < nsteps; t++) acc += forces[3 * (size_t)t + comp];
+  *J = acc / window;
+  const int* b = L->sbox;
+  const long m = (long)(b[3] - b[0]) * (b[4] - b[1]) * (b[5] - b[2]);
+  for (long k = 0; k < m; k++) dJds[k] = 0;
+  const double w = 1.0 / window;
+  for (int t = nsteps - 1; t >= 0; t--) {
+    const double wJ = t >= nsteps - window ? w : 0;
+    OR_FN(adj_step)(L, states + pop * (size_t)t, Tn, Tc, wJ, comp, dJds);
+    double* tmp = Tn; Tn = Tc; Tc = tmp;
+  }
+  free(states); free(forces); free(Tn); free(Tc);
+  return 0;
 }
 
 #undef OR_T

@@ -83,6 +83,8 @@ def lib() -> C.CDLL:
             "sample": ([C.c_void_p, C.c_double, C.c_double, C.c_double, _D], None),
             "is_solid": ([C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
             "step_sample": ([C.c_void_p, C.c_int, C.c_int, C.c_int], C.c_long),
+            "set_solid_fraction": ([C.c_void_p, C.POINTER(C.c_int), _D], C.c_int),
+            "adjoint": ([C.c_void_p, C.c_int, C.c_int, C.c_int, _D, _D], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, pfx + name)
@@ -295,3 +297,23 @@ class OracleLBM:
 
     def isSolid(self, x, y, z):
         return bool(self._fn("is_solid")(self.h, x, y, z))
+
+    # partial bounce-back and its adjoint (no reference counterpart)
+    def set_solid_fraction(self, box, s):
+        """box = (x0, y0, z0, x1, y1, z1), half-open; s indexed [z][y][x] over the box."""
+        b = (C.c_int * 6)(*[int(v) for v in box])
+        a = np.ascontiguousarray(s, np.float64).ravel()
+        self._sbox = tuple(int(v) for v in box)
+        rc = self._fn("set_solid_fraction")(self.h, b, _dp(a))
+        if rc != 0:
+            raise ValueError(f"oracle set_solid_fraction failed ({rc})")
+
+    def adjoint(self, nsteps: int, window: int, comp: int = 0):
+        """(J, dJ/ds over the box as [z][y][x]); the lattice advances nsteps."""
+        x0, y0, z0, x1, y1, z1 = self._sbox
+        g = np.empty((z1 - z0, y1 - y0, x1 - x0), np.float64)
+        J = C.c_double()
+        rc = self._fn("adjoint")(self.h, nsteps, window, comp, C.byref(J), _dp(g))
+        if rc != 0:
+            raise ValueError(f"oracle adjoint failed ({rc})")
+        return J.value, g

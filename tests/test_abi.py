@@ -45,7 +45,7 @@ def test_default_params_match_reference(wt_lib):
     p = _lib.default_params()
     assert p.u0 == 0.06 and p.tau == 0.5035 and p.les == 1 and p.csm == 0.14
     assert p.trt == 1 and p.lambda_ == 0.25 and p.side_bc == 0 and p.math == 0
-    assert p.kernel == 0 and p.f16_rounding == 1 and p.reserved == 0
+    assert p.kernel == 0 and p.f16_rounding == 0 and p.reserved == 0
 
 
 def test_create_rejects_bad_dims_on_host(wt_lib):

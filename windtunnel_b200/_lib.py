@@ -38,6 +38,8 @@ WT_KERNEL_DIRECT = 1
 WT_KERNEL_STAGED = 2
 WT_KERNEL_VECTOR = 3
 WT_KERNEL_PIPE = 4
+WT_KERNEL_X2 = 5
+WT_KERNEL_TMA = 6
 
 WT_ROUND_NEAREST = 0
 WT_ROUND_STOCHASTIC = 1
@@ -88,6 +90,16 @@ class wt_body_stats(C.Structure):
     ]
 
 
+class wt_adj_cfg(C.Structure):
+    _fields_ = [("nsteps", C.c_int32), ("window", C.c_int32), ("component", C.c_int32),
+                ("checkpoint", C.c_int32), ("reserved", C.c_int32 * 4)]
+
+
+class wt_adj_stats(C.Structure):
+    _fields_ = [("J", C.c_double), ("forward_ms", C.c_double), ("backward_ms", C.c_double),
+                ("device_bytes", C.c_int64), ("checkpoints", C.c_int32), ("segment", C.c_int32)]
+
+
 class WTError(RuntimeError):
     """A wt_* call returned a negative status."""
 
@@ -134,6 +146,8 @@ SIGNATURES = {
     "wt_is_solid": [_P, C.c_double, C.c_double, C.c_double, _I],
     "wt_get_stream": [_P, C.POINTER(_P)],
     "wt_get_launch_count": [_P, C.POINTER(C.c_int64)],
+    "wt_set_solid_fraction": [_P, _I, _D],
+    "wt_adjoint": [_P, C.POINTER(wt_adj_cfg), _D, C.POINTER(wt_adj_stats)],
 }
 _RESTYPES = {"wt_default_params": None, "wt_last_error": C.c_char_p}
 

@@ -76,6 +76,8 @@ void free_all(wt_lattice* h) {
   if (h->forces_host) cudaFreeHost(h->forces_host);
   if (h->err_host) cudaFreeHost(h->err_host);
   if (h->stream) cudaStreamDestroy(h->stream);
+  delete h->tma;
+  h->tma = nullptr;
 }
 
 int check_params(const wt_params* p) {
@@ -84,7 +86,7 @@ int check_params(const wt_params* p) {
   if (p->trt && !(p->lambda > 0)) return WT_ERR_ARG;
   if (p->side_bc != WT_SIDE_EQ && p->side_bc != WT_SIDE_FREESLIP) return WT_ERR_ARG;
   if (p->math != WT_MATH_FAST && p->math != WT_MATH_EXACT) return WT_ERR_ARG;
-  if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_PIPE) return WT_ERR_ARG;
+  if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_TMA) return WT_ERR_ARG;
   if (p->f16_rounding != WT_ROUND_NEAREST && p->f16_rounding != WT_ROUND_STOCHASTIC)
     return WT_ERR_ARG;
   if (p->reserved != 0) return WT_ERR_ARG;
@@ -153,6 +155,8 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
   double eq[19];
   wt::eq_u0_table(p.u0, eq);
   for (int q = 0; q < 19; q++) a.eq[q] = to_store<S>(eq[q]);
+  a.sfrac = h->sfrac;
+  for (int k = 0; k < 6; k++) a.sb[k] = h->sbox[k];
   return a;
 }
 
@@ -160,11 +164,11 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
 // direction block starts on a 16-byte boundary.
 bool staged_ok(const wt_lattice* h) { return h->nx % (int)(16 / h->elem) == 0; }
 
-enum class Path { Direct, Staged, Vector, Pipe };
+enum class Path { Direct, Staged, Vector, Pipe, X2, Tma, Pbb };
 
-template <class S, class L, class LS, class LV, class LP>
+template <class S, class L, class LS, class LV, class LP, class LX, class LT, class LB>
 void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged, LV launch_vec,
-               LP launch_pipe) {
+               LP launch_pipe, LX launch_x2, LT launch_tma, LB launch_pbb, double* forces_dev) {
   wt::StepArgs<S> a = make_args<S>(h);
   const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
   const bool wide = 19 * h->n >= (1LL << 31);
@@ -181,17 +185,47 @@ void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged,
         case Path::Staged: launch_staged(a, h->stream); break;
         case Path::Vector: launch_vec(a, wide, h->stream); break;
         case Path::Pipe: launch_pipe(a, wide, h->stream); break;
+        case Path::X2: launch_x2(a, wide, h->stream); break;
+        case Path::Tma: launch_tma(a, *h->tma, h->parity, h->stream); break;
+        case Path::Pbb: launch_pbb(a, grid, wide, h->stream); break;
         default: launch(a, grid, wide, h->stream); break;
       }
       h->launches++;
       h->parity ^= 1;
     }
-    wt::launch_force_reduce(h->part, (unsigned)h->nslots, chunk, h->forces_dev + 3 * (size_t)done,
+    wt::launch_force_reduce(h->part, (unsigned)h->nslots, chunk, forces_dev + 3 * (size_t)done,
                             h->stream);
     h->launches++;
     done += chunk;
   }
 }
+
+// True when the two-cells-per-thread packed kernel can run.
+bool x2_ok(const wt_lattice* h) {
+  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
+  const bool sr = h->storage == WT_STORE_F16DEV && h->p.f16_rounding == WT_ROUND_STOCHASTIC;
+  return !exact && !sr && h->nx % 2 == 0;
+}
+
+// The kernel WT_KERNEL_AUTO runs: the direct kernel for now.
+Path auto_path(const wt_lattice* h) {
+  (void)h;
+  return Path::Direct;
+}
+
+// True when the TMA tile kernel can run.
+bool tma_ok(const wt_lattice* h) {
+  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
+  const bool sr = h->storage == WT_STORE_F16DEV && h->p.f16_rounding == WT_ROUND_STOCHASTIC;
+  return !exact && !sr && h->tma != nullptr;
+}
+
+template <class S>
+void no_tma(const wt::StepArgs<S>&, const wt::TmaMaps&, int, cudaStream_t) {}
+
+int select_path(wt_lattice* h, Path* out);
+void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* forces_dev);
+int check_err_word(wt_lattice* h);
 
 // No vector / pipe kernel exists for the float64 collision; this stands in their slots.
 template <class S>
@@ -214,6 +248,15 @@ int rebuild_slots(wt_lattice* h) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   cudaFree(mark);
   if (e != cudaSuccess) return cuda_fail(h, e, "rebuild_slots");
+  if (h->sfrac) {
+    // every segment that touches the partial bounce-back box carries a force partial
+    const int* b = h->sbox;
+    const int nseg = (h->nx + 31) / 32;
+    for (int z = b[2]; z < b[5]; z++)
+      for (int y = b[1]; y < b[4]; y++)
+        for (int sx = b[0] / 32; sx <= (b[3] - 1) / 32; sx++)
+          hm[((size_t)z * h->ny + y) * nseg + sx] = 1;
+  }
   std::vector<int> slot(hm.size());
   int n = 0;
   for (size_t w = 0; w < hm.size(); w++) slot[w] = hm[w] ? n++ : -1;
@@ -251,7 +294,7 @@ void wt_default_params(wt_params* p) {
   p->side_bc = WT_SIDE_EQ;
   p->math = WT_MATH_FAST;
   p->kernel = WT_KERNEL_AUTO;
-  p->f16_rounding = WT_ROUND_STOCHASTIC;
+  p->f16_rounding = WT_ROUND_NEAREST;
 }
 
 const char* wt_last_error(const wt_lattice* h) {
@@ -323,6 +366,14 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
     free_all(h);
     delete h;
     return WT_ERR_CUDA;
+  }
+  if (wt::tma_supported(storage, nx)) {
+    // tensor maps of the TMA tile kernel over both population buffers (they never move)
+    h->tma = new wt::TmaMaps();
+    if (!wt::make_tma_maps(storage, h->buf, nx, ny, nz, h->tma)) {
+      delete h->tma;
+      h->tma = nullptr;
+    }
   }
   *out = h;
   return WT_OK;
@@ -529,9 +580,39 @@ int wt_step(wt_lattice* h, int nsteps, double* forces) {
   if (c != WT_OK) return c;
   WT_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(unsigned), h->stream));
   WT_CUDA(h, cudaMemsetAsync(h->diag_dev, 0, 4 * sizeof(long long), h->stream));
+  Path path = Path::Direct;
+  c = select_path(h, &path);
+  if (c != WT_OK) return c;
+  dispatch_steps(h, nsteps, path, h->forces_dev);
+  WT_CUDA(h, cudaGetLastError());
+  WT_CUDA(h, cudaMemcpyAsync(h->forces_host, h->forces_dev, sizeof(double) * 3 * (size_t)nsteps,
+                             cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaMemcpyAsync(h->err_host, h->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             h->stream));
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->steps += nsteps;
+  const double* last = h->forces_host + 3 * (size_t)(nsteps - 1);
+  h->force[0] = last[0]; h->force[1] = last[1]; h->force[2] = last[2];
+  if (forces) memcpy(forces, h->forces_host, sizeof(double) * 3 * (size_t)nsteps);
+  return check_err_word(h);
+}
+
+}  // extern "C"
+
+namespace {
+
+// The kernel a wt_step call runs, from the handle's parameters.
+int select_path(wt_lattice* h, Path* out) {
   const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
   const bool vec_ok = !exact && h->nx % 2 == 0;
   Path path = Path::Direct;
+  if (h->sfrac) {
+    if (h->p.kernel != WT_KERNEL_AUTO && h->p.kernel != WT_KERNEL_DIRECT)
+      return fail(h, WT_ERR_UNSUPPORTED,
+                  "a lattice with a solid-fraction field runs the direct kernel only");
+    *out = Path::Pbb;
+    return WT_OK;
+  }
   switch (h->p.kernel) {
     case WT_KERNEL_STAGED:
       if (!staged_ok(h))
@@ -550,40 +631,60 @@ int wt_step(wt_lattice* h, int nsteps, double* forces) {
         return fail(h, WT_ERR_UNSUPPORTED, "the pipe kernel runs the float32 collision only");
       path = Path::Pipe;
       break;
-    case WT_KERNEL_AUTO:   // the fastest measured on B200 for every form
-      path = Path::Direct;
+    case WT_KERNEL_X2:
+      if (!x2_ok(h))
+        return fail(h, WT_ERR_UNSUPPORTED,
+                    "the x2 kernel needs the float32 collision, an even nx and nearest "
+                    "rounding for half storage");
+      path = Path::X2;
+      break;
+    case WT_KERNEL_TMA:
+      if (!tma_ok(h))
+        return fail(h, WT_ERR_UNSUPPORTED,
+                    "the TMA kernel needs the float32 collision, nx a multiple of 16 bytes / "
+                    "element (4 float32, 8 half) and nearest rounding for half storage");
+      path = Path::Tma;
+      break;
+    case WT_KERNEL_AUTO:
+      path = auto_path(h);
       break;
     default:
       break;
   }
+  *out = path;
+  return WT_OK;
+}
+
+// Run nsteps steps of the chosen kernel; per-step forces land in forces_dev.
+void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* forces_dev) {
+  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
   switch (h->storage) {
     case WT_STORE_F32:
       if (exact) run_steps<float>(h, nsteps, path, wt::launch_step_f32_exact,
-                                  wt::launch_staged_f32_exact, no_vec<float>, no_vec<float>);
+                                  wt::launch_staged_f32_exact, no_vec<float>, no_vec<float>,
+                                  no_vec<float>, no_tma<float>, wt::launch_pbb_f32_exact,
+                                  forces_dev);
       else run_steps<float>(h, nsteps, path, wt::launch_step_f32_fast, wt::launch_staged_f32_fast,
-                            wt::launch_vec_f32, wt::launch_pipe_f32);
+                            wt::launch_vec_f32, wt::launch_pipe_f32, wt::launch_x2_f32,
+                            wt::launch_tma_f32, wt::launch_pbb_f32_fast, forces_dev);
       break;
     case WT_STORE_F16DEV:
       run_steps<__half>(h, nsteps, path, wt::launch_step_f16_fast, wt::launch_staged_f16_fast,
-                        wt::launch_vec_f16, wt::launch_pipe_f16);
+                        wt::launch_vec_f16, wt::launch_pipe_f16, wt::launch_x2_f16,
+                        wt::launch_tma_f16, wt::launch_pbb_f16_fast, forces_dev);
       break;
     default:
       run_steps<double>(h, nsteps, path, wt::launch_step_f64_exact, wt::launch_staged_f64_exact,
-                        no_vec<double>, no_vec<double>);
+                        no_vec<double>, no_vec<double>, no_vec<double>, no_tma<double>,
+                        wt::launch_pbb_f64_exact, forces_dev);
       break;
   }
-  WT_CUDA(h, cudaGetLastError());
-  WT_CUDA(h, cudaMemcpyAsync(h->forces_host, h->forces_dev, sizeof(double) * 3 * (size_t)nsteps,
-                             cudaMemcpyDeviceToHost, h->stream));
-  WT_CUDA(h, cudaMemcpyAsync(h->err_host, h->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost,
-                             h->stream));
-  WT_CUDA(h, cudaStreamSynchronize(h->stream));
-  h->steps += nsteps;
-  const double* last = h->forces_host + 3 * (size_t)(nsteps - 1);
-  h->force[0] = last[0]; h->force[1] = last[1]; h->force[2] = last[2];
-  if (forces) memcpy(forces, h->forces_host, sizeof(double) * 3 * (size_t)nsteps);
+}
+
+// Status of the error word the last steps left in h->err_host.
+int check_err_word(wt_lattice* h) {
   if (*h->err_host & 4u)
-    return fail(h, WT_ERR_TIMEOUT, "a staged row copy did not complete within its wait budget");
+    return fail(h, WT_ERR_TIMEOUT, "a staged copy did not complete within its wait budget");
   if (*h->err_host & 8u) {
     long long d[4] = {0, 0, 0, 0};
     cudaMemcpy(d, h->diag_dev, sizeof(d), cudaMemcpyDeviceToHost);
@@ -600,6 +701,10 @@ int wt_step(wt_lattice* h, int nsteps, double* forces) {
     return fail(h, WT_ERR_DIVERGED, "a step produced a non-finite or non-positive density");
   return WT_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int wt_get_force(const wt_lattice* h, double out[3]) {
   if (!h || !out) return WT_ERR_ARG;
@@ -829,6 +934,182 @@ int wt_get_launch_count(const wt_lattice* h, int64_t* count) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Partial bounce-back field and the discrete adjoint of the step.
+
+extern "C" int wt_set_solid_fraction(wt_lattice* h, const int box[6], const double* s) {
+  if (!h) return WT_ERR_ARG;
+  if (h->sfrac) {
+    cudaFree(h->sfrac);
+    h->sfrac = nullptr;
+  }
+  for (int k = 0; k < 6; k++) h->sbox[k] = 0;
+  if (!box) return rebuild_slots(h);
+  const int x0 = box[0], y0 = box[1], z0 = box[2], x1 = box[3], y1 = box[4], z1 = box[5];
+  if (!s || x0 < 0 || y0 < 0 || z0 < 0 || x1 > h->nx || y1 > h->ny || z1 > h->nz || x1 <= x0 ||
+      y1 <= y0 || z1 <= z0)
+    return fail(h, WT_ERR_ARG, "solid-fraction box must be non-empty and inside the lattice, "
+                               "with values");
+  const size_t m = (size_t)(x1 - x0) * (y1 - y0) * (z1 - z0);
+  for (size_t k = 0; k < m; k++)
+    if (!std::isfinite(s[k]) || s[k] < 0.0 || s[k] > 1.0)
+      return fail(h, WT_ERR_ARG, "solid fractions must lie in [0, 1]");
+  if (cudaMalloc((void**)&h->sfrac, sizeof(double) * m) != cudaSuccess) {
+    h->sfrac = nullptr;
+    return fail(h, WT_ERR_OOM, "cannot allocate the solid-fraction field");
+  }
+  WT_CUDA(h, cudaMemcpy(h->sfrac, s, sizeof(double) * m, cudaMemcpyHostToDevice));
+  for (int k = 0; k < 6; k++) h->sbox[k] = box[k];
+  return rebuild_slots(h);
+}
+
+namespace {
+
+// Device buffers of one adjoint run, released on every exit path.
+struct AdjBuffers {
+  std::vector<void*> ptrs;
+  size_t bytes = 0;
+  void* get(size_t n) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, n) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    bytes += n;
+    return p;
+  }
+  ~AdjBuffers() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+};
+
+template <class S, class T, class LA, class LP>
+int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_adj_stats* st,
+                LA launch_adj, LP launch_pbb) {
+  const int N = cfg.nsteps, W = cfg.window;
+  const size_t pop = (size_t)h->n * 19 * sizeof(S);
+  const size_t tsz = (size_t)h->n * 19 * sizeof(T);
+  const int ncp = (N + C - 1) / C;
+  const int* b = h->sbox;
+  const size_t nbox = (size_t)(b[3] - b[0]) * (b[4] - b[1]) * (b[5] - b[2]);
+  AdjBuffers mem;
+  S* cps = (S*)mem.get(pop * (size_t)ncp);          // checkpoints S^{kC}
+  S* seg = (S*)mem.get(pop * (size_t)C);            // states of one segment
+  T* Tbuf[2] = {(T*)mem.get(tsz), (T*)mem.get(tsz)};
+  double* ds = (double*)mem.get(sizeof(double) * nbox);
+  double* fdev = (double*)mem.get(sizeof(double) * 3 * (size_t)N);
+  if (!cps || !seg || !Tbuf[0] || !Tbuf[1] || !ds || !fdev)
+    return fail(h, WT_ERR_OOM, "cannot allocate the adjoint's checkpoints (" +
+                                   std::to_string((pop * (size_t)(ncp + C) + 2 * tsz) >> 20) +
+                                   " MiB)");
+  cudaEvent_t e0, e1, e2;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventCreate(&e2);
+  WT_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(unsigned), h->stream));
+  cudaEventRecord(e0, h->stream);
+  // forward sweep: a checkpoint every C steps, the force series for J
+  for (int k = 0; k < ncp; k++) {
+    WT_CUDA(h, cudaMemcpyAsync(cps + (size_t)k * (pop / sizeof(S)), h->buf[h->parity], pop,
+                               cudaMemcpyDeviceToDevice, h->stream));
+    const int n = std::min(C, N - k * C);
+    dispatch_steps(h, n, Path::Pbb, fdev + 3 * (size_t)k * C);
+  }
+  cudaEventRecord(e1, h->stream);
+  // backward sweep, segment by segment: recompute the segment's states from
+  // its checkpoint, then run its adjoint steps last to first
+  WT_CUDA(h, cudaMemsetAsync(Tbuf[0], 0, tsz, h->stream));
+  WT_CUDA(h, cudaMemsetAsync(ds, 0, sizeof(double) * nbox, h->stream));
+  int cur = 0;   // Tbuf[cur] holds T^{t+1}
+  wt::StepArgs<S> a = make_args<S>(h);
+  a.write_fields = 0;
+  a.part = h->part;   // force partials of recomputed steps are not reduced
+  const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
+  const bool wide = 19 * h->n >= (1LL << 31);
+  for (int k = ncp - 1; k >= 0; k--) {
+    const int t0 = k * C, n = std::min(C, N - t0);
+    WT_CUDA(h, cudaMemcpyAsync(seg, cps + (size_t)k * (pop / sizeof(S)), pop,
+                               cudaMemcpyDeviceToDevice, h->stream));
+    for (int j = 0; j + 1 < n; j++) {
+      a.F = seg + (size_t)j * (pop / sizeof(S));
+      a.G = seg + (size_t)(j + 1) * (pop / sizeof(S));
+      launch_pbb(a, grid, wide, h->stream);
+      h->launches++;
+    }
+    for (int t = t0 + n - 1; t >= t0; t--) {
+      a.F = seg + (size_t)(t - t0) * (pop / sizeof(S));
+      const double wJ = t >= N - W ? 1.0 / W : 0.0;
+      launch_adj(a, Tbuf[cur], Tbuf[cur ^ 1], ds, wJ, cfg.component, h->stream);
+      h->launches++;
+      cur ^= 1;
+    }
+  }
+  cudaEventRecord(e2, h->stream);
+  WT_CUDA(h, cudaGetLastError());
+  std::vector<double> fh(3 * (size_t)N);
+  WT_CUDA(h, cudaMemcpyAsync(fh.data(), fdev, sizeof(double) * fh.size(), cudaMemcpyDeviceToHost,
+                             h->stream));
+  WT_CUDA(h, cudaMemcpyAsync(dJds, ds, sizeof(double) * nbox, cudaMemcpyDeviceToHost, h->stream));
+  WT_CUDA(h, cudaMemcpyAsync(h->err_host, h->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             h->stream));
+  WT_CUDA(h, cudaStreamSynchronize(h->stream));
+  float fwd_ms = 0, bwd_ms = 0;
+  cudaEventElapsedTime(&fwd_ms, e0, e1);
+  cudaEventElapsedTime(&bwd_ms, e1, e2);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  double J = 0;
+  for (int t = N - W; t < N; t++) J += fh[3 * (size_t)t + cfg.component];
+  J /= W;
+  h->steps += N;
+  h->force[0] = fh[3 * (size_t)(N - 1)];
+  h->force[1] = fh[3 * (size_t)(N - 1) + 1];
+  h->force[2] = fh[3 * (size_t)(N - 1) + 2];
+  if (st) {
+    st->J = J;
+    st->forward_ms = fwd_ms;
+    st->backward_ms = bwd_ms;
+    st->device_bytes = (int64_t)mem.bytes;
+    st->checkpoints = ncp;
+    st->segment = C;
+  }
+  return check_err_word(h);
+}
+
+}  // namespace
+
+extern "C" int wt_adjoint(wt_lattice* h, const wt_adj_cfg* cfg, double* dJds, wt_adj_stats* st) {
+  if (!h) return WT_ERR_ARG;
+  if (!cfg || !dJds) return fail(h, WT_ERR_ARG, "cfg and dJds are required");
+  if (!h->sfrac) return fail(h, WT_ERR_STATE, "set a solid-fraction field first");
+  if (cfg->nsteps < 1 || cfg->window < 1 || cfg->window > cfg->nsteps || cfg->component < 0 ||
+      cfg->component > 2 || cfg->checkpoint < 0)
+    return fail(h, WT_ERR_ARG, "need nsteps >= 1, 1 <= window <= nsteps, component 0..2, "
+                               "checkpoint >= 0");
+  if (h->p.moving_walls)
+    return fail(h, WT_ERR_UNSUPPORTED, "the adjoint supports stationary walls only");
+  if (h->p.kernel != WT_KERNEL_AUTO && h->p.kernel != WT_KERNEL_DIRECT)
+    return fail(h, WT_ERR_UNSUPPORTED, "the adjoint runs the direct kernel");
+  int C = cfg->checkpoint;
+  if (C == 0) C = std::max(1, (int)std::ceil(std::sqrt((double)cfg->nsteps)));
+  C = std::min(C, cfg->nsteps);
+  int c = grow_forces(h, 1);
+  if (c != WT_OK) return c;
+  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
+  switch (h->storage) {
+    case WT_STORE_F32:
+      if (exact) return adjoint_run<float, double>(h, *cfg, C, dJds, st, wt::launch_adj_f32x,
+                                                   wt::launch_pbb_f32_exact);
+      return adjoint_run<float, float>(h, *cfg, C, dJds, st, wt::launch_adj_f32,
+                                       wt::launch_pbb_f32_fast);
+    case WT_STORE_F16DEV:
+      return adjoint_run<__half, float>(h, *cfg, C, dJds, st, wt::launch_adj_f16,
+                                        wt::launch_pbb_f16_fast);
+    default:
+      return adjoint_run<double, double>(h, *cfg, C, dJds, st, wt::launch_adj_f64,
+                                         wt::launch_pbb_f64_exact);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // wt_step_noalloc: the step for callers that must not allocate device memory
 // while they run, such as a host whose own memory pool has already claimed
 // the device's memory, or a host stepping inside a frame loop that must not
@@ -912,6 +1193,8 @@ extern "C" int wt_step_noalloc(wt_lattice* h, int nsteps, double* forces) {
                     " its fixed scratch holds; use wt_step");
   if (h->p.kernel != WT_KERNEL_AUTO && h->p.kernel != WT_KERNEL_DIRECT)
     return fail(h, WT_ERR_UNSUPPORTED, "wt_step_noalloc runs the direct kernel only");
+  if (h->sfrac)
+    return fail(h, WT_ERR_UNSUPPORTED, "wt_step_noalloc does not run partial bounce-back");
   int dev = -1;
   WT_CUDA(h, cudaGetDevice(&dev));
   if (dev != h->device)

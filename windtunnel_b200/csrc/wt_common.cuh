@@ -2,6 +2,7 @@
 // parameter blocks shared by every kernel of libwt.so.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -130,6 +131,20 @@ struct StepArgs {
   int gx;              // x-segments (units) per row
   long long units;     // gx*ny*nz
   S eq[Q];             // equilibrium deviation at rho=1, u=(u0,0,0), rounded to S
+  const double* sfrac; // partial bounce-back: solid fraction on the box sb (x fastest), or null
+  int sb[6];           // its half-open box x0, y0, z0, x1, y1, z1
+};
+
+// The four tensor maps of a lattice for the TMA step kernel: loads (box of
+// (tile width + 2 * halo) x tile rows) and stores (box tile width x tile rows)
+// over population buffers A and B, dims (nx, ny, nz, 19).
+struct TmaMaps {
+  CUtensorMap ld[2];
+  CUtensorMap st[2];
+  // tile geometry: tx cells x ty rows per tile; loaded boxes bw = tx + 2h wide
+  // starting h cells left of the tile; per-direction slot pitches in shared
+  // memory (elements, 128-byte multiples); tiles per row and per plane
+  int tx, ty, bw, h, in_slot, out_slot, gx, gy;
 };
 
 // Block shape of the fused step: one thread per cell along x.

@@ -40,6 +40,9 @@ struct wt_lattice {
   unsigned* err_dev = nullptr;
   unsigned* err_host = nullptr;  // pinned
   long long* diag_dev = nullptr; // first rejected staged copy {kind, q, unit, offset}
+  wt::TmaMaps* tma = nullptr;    // tensor maps of the TMA tile kernel (host copy), or null
+  double* sfrac = nullptr;       // partial bounce-back solid fraction on sbox (device), or null
+  int sbox[6] = {0, 0, 0, 0, 0, 0};
   // voxelize statistics scratch
   uint8_t* col = nullptr;        // ny*nz frontal projection
   uint8_t* plan = nullptr;       // nx*nz planform projection
@@ -66,6 +69,33 @@ void launch_step_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cuda
 // Vector (two cells per thread) step launchers, float32 collision; nx even.
 void launch_vec_f32(const StepArgs<float>& a, bool wide, cudaStream_t s);
 void launch_vec_f16(const StepArgs<__half>& a, bool wide, cudaStream_t s);
+
+// Two-cells-per-thread step launchers with the packed float32x2 collision; nx even.
+void launch_x2_f32(const StepArgs<float>& a, bool wide, cudaStream_t s);
+void launch_x2_f16(const StepArgs<__half>& a, bool wide, cudaStream_t s);
+
+// TMA tile step (tensor-map loads and stores through shared memory), float32
+// collision, float32 or half storage with nx a multiple of 16 bytes.
+bool tma_supported(int storage, int nx);
+bool make_tma_maps(int storage, void* const buf[2], int nx, int ny, int nz, TmaMaps* out);
+void launch_tma_f32(const StepArgs<float>& a, const TmaMaps& m, int ld_buf, cudaStream_t s);
+void launch_tma_f16(const StepArgs<__half>& a, const TmaMaps& m, int ld_buf, cudaStream_t s);
+
+// Partial bounce-back step (direct, one thread per cell) and one step of
+// its discrete adjoint. The adjoint arithmetic is float64 for float64
+// storage or the exact collision, float32 otherwise.
+void launch_pbb_f32_fast(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_pbb_f16_fast(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_pbb_f32_exact(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_pbb_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_adj_f32(const StepArgs<float>& a, const float* Tn, float* Tc, double* ds, double wJ,
+                    int comp, cudaStream_t s);
+void launch_adj_f16(const StepArgs<__half>& a, const float* Tn, float* Tc, double* ds, double wJ,
+                    int comp, cudaStream_t s);
+void launch_adj_f32x(const StepArgs<float>& a, const double* Tn, double* Tc, double* ds,
+                     double wJ, int comp, cudaStream_t s);
+void launch_adj_f64(const StepArgs<double>& a, const double* Tn, double* Tc, double* ds,
+                    double wJ, int comp, cudaStream_t s);
 
 // Software-pipelined step launchers, float32 collision.
 void launch_pipe_f32(const StepArgs<float>& a, bool wide, cudaStream_t s);

@@ -8,6 +8,7 @@
 
 #include "wt_internal.h"
 #include "wt_staged_launch.cuh"
+#include "wt_pbb.cuh"
 
 namespace wt {
 
@@ -19,6 +20,28 @@ void launch_step_f32_exact(const StepArgs<float>& a, dim3 grid, bool wide, cudaS
 void launch_step_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cudaStream_t s) {
   if (wide) k_step<double, true, long long><<<grid, STEP_BX, 0, s>>>(a);
   else k_step<double, true, int><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+void launch_pbb_f32_exact(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s) {
+  if (wide) k_step_pbb<float, true, long long><<<grid, STEP_BX, 0, s>>>(a);
+  else k_step_pbb<float, true, int><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+void launch_pbb_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cudaStream_t s) {
+  if (wide) k_step_pbb<double, true, long long><<<grid, STEP_BX, 0, s>>>(a);
+  else k_step_pbb<double, true, int><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+void launch_adj_f32x(const StepArgs<float>& a, const double* Tn, double* Tc, double* ds,
+                     double wJ, int comp, cudaStream_t s) {
+  AdjArgs<double> j{Tn, Tc, ds, wJ, comp};
+  k_adjoint<float, double><<<step_grid(a.nx, a.ny, a.nz), STEP_BX, 0, s>>>(a, j);
+}
+
+void launch_adj_f64(const StepArgs<double>& a, const double* Tn, double* Tc, double* ds,
+                    double wJ, int comp, cudaStream_t s) {
+  AdjArgs<double> j{Tn, Tc, ds, wJ, comp};
+  k_adjoint<double, double><<<step_grid(a.nx, a.ny, a.nz), STEP_BX, 0, s>>>(a, j);
 }
 
 void launch_staged_f32_exact(const StepArgs<float>& a, cudaStream_t s) {

@@ -1,0 +1,391 @@
+// wt_pbb.cuh — partial bounce-back step and its discrete adjoint.
+//
+// Partial bounce-back (no counterpart in the reference): a fluid cell with
+// solid fraction s in [0, 1] stores
+//     g_q = (1 - s) gc_q + s f_opp(q)
+// where f are its pulled populations and gc the collided ones, and adds
+//     s * sum_q c_q (gc_q - f_opp(q))
+// to the momentum-exchange force. s = 0 is the plain step; s = 1 reverses
+// every population of the cell. The field lives on a box of cells
+// (StepArgs::sfrac, float64, x fastest).
+//
+// k_step_pbb is k_step (wt_step.cuh) with the collision written as a plain
+// per-direction sequence (cell_fw) so that the collided values can be blended
+// before they are rounded to the storage type; its operation order is that of
+// js/lbm.js:377-460, so with EXACT it reproduces the reference arithmetic
+// bit for bit where s = 0.
+//
+// k_adjoint is one step of the discrete adjoint, run backwards in time over
+// stored forward states. T^t[q][i] is dJ/d(value pulled by link q of cell i at
+// step t). The adjoint of the population stored at location (q, j) after step
+// t is the sum of T^{t+1} over the links that pull it at step t+1: the plain
+// consumer j + c_q, the cell j itself when that neighbour is solid
+// (bounce-back), and the mirrored consumer when that neighbour is a free-slip
+// side plane; the outlet column x = nx-1 is a copy of column nx-2, so its
+// adjoint is added to column nx-2's. Cells that do not pull (inlet, outlet,
+// side planes, solids) write zero rows. Every adjoint step is therefore a
+// pull-shaped pass like the forward step: per cell it gathers 19 adjoint
+// values, recomputes the forward collision from the stored state, and writes
+// the 19 adjoint values of its pulled links, accumulating dJ/ds on the box.
+#pragma once
+
+#include "wt_step.cuh"
+
+namespace wt {
+
+// Forward collision of one cell and the intermediates its adjoint needs, in
+// the operation order of js/lbm.js:377-460 (and of collide_exact).
+template <class T>
+struct CellFw {
+  T f[Q], gc[Q], n[Q];
+  T r, inv, jx, jy, jz, vx, vy, vz, usq, A, r3, r45;
+  T pxx, pyy, pzz, pxy, pxz, pyz, mag, R, tauEff, om, omm;
+};
+
+template <class T, class S>
+__device__ __forceinline__ void cell_fw(const StepArgs<S>& a, CellFw<T>& c) {
+  const T* f = c.f;
+  const T dr = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] + f[11] +
+               f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
+  const T r = (T)1 + dr;
+  const T inv = (T)1 / r;
+  const T jx = f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[11] - f[12] + f[13] - f[14];
+  const T jy = f[3] - f[4] + f[7] - f[8] - f[9] + f[10] + f[15] - f[16] + f[17] - f[18];
+  const T jz = f[5] - f[6] + f[11] - f[12] - f[13] + f[14] + f[15] - f[16] - f[17] + f[18];
+  const T vx = jx * inv, vy = jy * inv, vz = jz * inv;
+  const T usq = vx * vx + vy * vy + vz * vz;
+  const T A = dr - r * (T)1.5 * usq;
+  const T r3 = (T)3 * r, r45 = (T)4.5 * r;
+  T e[Q];
+  e[0] = (T)wq(0) * A;
+#pragma unroll
+  for (int q = 1; q < Q; q++) {
+    const T cv = (T)ex(q) * vx + (T)ey(q) * vy + (T)ez(q) * vz;
+    e[q] = (T)wq(q) * (A + r3 * cv + r45 * cv * cv);
+  }
+#pragma unroll
+  for (int q = 0; q < Q; q++) c.n[q] = f[q] - e[q];
+  const T* n = c.n;
+  const T tau0 = (T)a.tau0;
+  T om = (T)1 / tau0, tauEff = tau0;
+  c.pxx = c.pyy = c.pzz = c.pxy = c.pxz = c.pyz = c.mag = c.R = (T)0;
+  if (a.les) {
+    c.pxx = n[1] + n[2] + n[7] + n[8] + n[9] + n[10] + n[11] + n[12] + n[13] + n[14];
+    c.pyy = n[3] + n[4] + n[7] + n[8] + n[9] + n[10] + n[15] + n[16] + n[17] + n[18];
+    c.pzz = n[5] + n[6] + n[11] + n[12] + n[13] + n[14] + n[15] + n[16] + n[17] + n[18];
+    c.pxy = n[7] + n[8] - n[9] - n[10];
+    c.pxz = n[11] + n[12] - n[13] - n[14];
+    c.pyz = n[15] + n[16] - n[17] - n[18];
+    c.mag = sqrt((T)2 * (c.pxx * c.pxx + c.pyy * c.pyy + c.pzz * c.pzz +
+                         (T)2 * (c.pxy * c.pxy + c.pxz * c.pxz + c.pyz * c.pyz)));
+    const T SQ18 = (T)(18 * 1.4142135623730951);
+    c.R = sqrt(tau0 * tau0 + SQ18 * (T)a.cs2 * c.mag * inv);
+    tauEff = (T)0.5 * (tau0 + c.R);
+    om = (T)1 / tauEff;
+  }
+  const T omm = a.trt ? (T)1 / ((T)0.5 + (T)a.lam / (tauEff - (T)0.5)) : om;
+  c.gc[0] = f[0] - om * (f[0] - e[0]);
+#pragma unroll
+  for (int k = 1; k < Q; k += 2) {
+    const T sp = (T)0.5 * (n[k] + n[k + 1]), sm = (T)0.5 * (n[k] - n[k + 1]);
+    c.gc[k] = f[k] - om * sp - omm * sm;
+    c.gc[k + 1] = f[k + 1] - om * sp + omm * sm;
+  }
+  c.r = r; c.inv = inv; c.jx = jx; c.jy = jy; c.jz = jz; c.vx = vx; c.vy = vy; c.vz = vz;
+  c.usq = usq; c.A = A; c.r3 = r3; c.r45 = r45; c.tauEff = tauEff; c.om = om; c.omm = omm;
+}
+
+// fb += (d gc / d f)^T a for the collision of cell_fw.
+template <class T, class S>
+__device__ __forceinline__ void cell_vjp(const StepArgs<S>& a, const CellFw<T>& c, const T (&ab)[Q],
+                                         T (&fb)[Q]) {
+  const T* n = c.n;
+  T nb[Q];
+#pragma unroll
+  for (int q = 0; q < Q; q++) fb[q] += ab[q];
+  T omb = -(ab[0] * n[0]);
+  T ommb = (T)0;
+  nb[0] = -(c.om * ab[0]);
+#pragma unroll
+  for (int k = 1; k < Q; k += 2) {
+    const T sp = (T)0.5 * (n[k] + n[k + 1]), sm = (T)0.5 * (n[k] - n[k + 1]);
+    const T as = ab[k] + ab[k + 1], ad = ab[k] - ab[k + 1];
+    omb -= as * sp;
+    ommb -= ad * sm;
+    const T spb = -(c.om * as), smb = -(c.omm * ad);
+    nb[k] = (T)0.5 * (spb + smb);
+    nb[k + 1] = (T)0.5 * (spb - smb);
+  }
+  T invb = (T)0;
+  if (a.les) {
+    T teb;
+    if (a.trt) {
+      const T tm = c.tauEff - (T)0.5;
+      teb = ommb * (c.omm * c.omm * (T)a.lam / (tm * tm)) - omb * (c.om * c.om);
+    } else {
+      teb = -(omb + ommb) * (c.om * c.om);
+    }
+    const T Rb = (T)0.5 * teb;
+    const T Xb = Rb / ((T)2 * c.R);
+    const T K = (T)(18 * 1.4142135623730951) * (T)a.cs2;
+    const T magb = Xb * K * c.inv;
+    invb += Xb * K * c.mag;
+    const T Qb = c.mag > (T)0 ? magb / c.mag : (T)0;
+    const T pxxb = (T)2 * c.pxx * Qb, pyyb = (T)2 * c.pyy * Qb, pzzb = (T)2 * c.pzz * Qb;
+    const T pxyb = (T)4 * c.pxy * Qb, pxzb = (T)4 * c.pxz * Qb, pyzb = (T)4 * c.pyz * Qb;
+    nb[1] += pxxb; nb[2] += pxxb;
+    nb[3] += pyyb; nb[4] += pyyb;
+    nb[5] += pzzb; nb[6] += pzzb;
+    nb[7] += pxxb + pyyb + pxyb; nb[8] += pxxb + pyyb + pxyb;
+    nb[9] += pxxb + pyyb - pxyb; nb[10] += pxxb + pyyb - pxyb;
+    nb[11] += pxxb + pzzb + pxzb; nb[12] += pxxb + pzzb + pxzb;
+    nb[13] += pxxb + pzzb - pxzb; nb[14] += pxxb + pzzb - pxzb;
+    nb[15] += pyyb + pzzb + pyzb; nb[16] += pyyb + pzzb + pyzb;
+    nb[17] += pyyb + pzzb - pyzb; nb[18] += pyyb + pzzb - pyzb;
+  }
+  T Ab = (T)0, r3b = (T)0, r45b = (T)0, vxb = (T)0, vyb = (T)0, vzb = (T)0;
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    fb[q] += nb[q];
+    const T eb = -nb[q];
+    Ab += (T)wq(q) * eb;
+    if (q > 0) {
+      const T cv = (T)ex(q) * c.vx + (T)ey(q) * c.vy + (T)ez(q) * c.vz;
+      const T web = (T)wq(q) * eb;
+      r3b += web * cv;
+      r45b += web * (cv * cv);
+      const T cvb = web * (c.r3 + (T)2 * c.r45 * cv);
+      vxb += (T)ex(q) * cvb; vyb += (T)ey(q) * cvb; vzb += (T)ez(q) * cvb;
+    }
+  }
+  T drb = Ab;
+  T rb = (T)3 * r3b + (T)4.5 * r45b - (T)1.5 * c.usq * Ab;
+  const T usqb = -(c.r * (T)1.5 * Ab);
+  vxb += (T)2 * c.vx * usqb; vyb += (T)2 * c.vy * usqb; vzb += (T)2 * c.vz * usqb;
+  invb += vxb * c.jx + vyb * c.jy + vzb * c.jz;
+  const T jxb = vxb * c.inv, jyb = vyb * c.inv, jzb = vzb * c.inv;
+  rb -= c.inv * c.inv * invb;
+  drb += rb;
+#pragma unroll
+  for (int q = 0; q < Q; q++)
+    fb[q] += drb + ((T)ex(q) * jxb + (T)ey(q) * jyb + (T)ez(q) * jzb);
+}
+
+// Solid fraction of cell (x, y, z); 0 outside the box.
+template <class S>
+__device__ __forceinline__ double sfrac_at(const StepArgs<S>& a, int x, int y, int z) {
+  if (!a.sfrac) return 0.0;
+  if (x < a.sb[0] || x >= a.sb[3] || y < a.sb[1] || y >= a.sb[4] || z < a.sb[2] || z >= a.sb[5])
+    return 0.0;
+  return a.sfrac[(x - a.sb[0]) + (long long)(a.sb[3] - a.sb[0]) *
+                                     ((y - a.sb[1]) + (long long)(a.sb[4] - a.sb[1]) * (z - a.sb[2]))];
+}
+
+template <class T, class S>
+__device__ __forceinline__ S to_store(T v) {
+  if constexpr (std::is_same<T, double>::value) return Store<S>::from_d(v);
+  else return Store<S>::from_f(v);
+}
+
+// The fused step with partial bounce-back: k_step's categories and boundary
+// rules, the collision of cell_fw, then the blend and its force.
+template <class S, bool EXACT, class IDX>
+__global__ void __launch_bounds__(STEP_BX) k_step_pbb(const __grid_constant__ StepArgs<S> a) {
+  using M = typename std::conditional<EXACT, double, float>::type;
+  const int x = blockIdx.x * STEP_BX + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z;
+  const long long i = (long long)x + (long long)a.nx * y + a.nxy * z;
+  double Fx = 0, Fy = 0, Fz = 0;
+  // Every 32-cell segment that touches the box owns a force slot and must
+  // write it every step (zeros where nothing is exchanged): cells of the box
+  // take part in the warp's partial whatever their category.
+  bool near_cell = x < a.nx && x >= a.sb[0] && x < a.sb[3] && y >= a.sb[1] && y < a.sb[4] &&
+                   z >= a.sb[2] && z < a.sb[5];
+  if (x < a.nx - 1) {
+    int cat;
+    uint8_t fl = 0;
+    const bool dup = (x == a.nx - 2);
+    if (x == 0) {
+      cat = CAT_EQ;
+    } else {
+      fl = a.flags[i];
+      if (z == 0 || z == a.nz - 1 || y == a.ny - 1) cat = CAT_EQ;
+      else if (fl & FLAG_SOLID_MASK) cat = CAT_KEEP;
+      else if (y == 0) cat = CAT_EQ;
+      else cat = CAT_FLUID;
+    }
+    S* Gi = a.G + i;
+    if (cat == CAT_FLUID) {
+      CellFw<M> c;
+      const bool wall = (fl & FLAG_NEAR) != 0;
+      near_cell = near_cell || wall;
+      const bool shell = a.freeslip && (y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2);
+      const S* Fi = a.F + i;
+#pragma unroll
+      for (int q = 0; q < Q; q++) c.f[q] = ld<M>(Fi[(IDX)a.src[q]]);
+      if (wall || shell) patch_special<S, M>(a, i, x, y, z, shell, c.f, Fx, Fy, Fz);
+      cell_fw<M>(a, c);
+      if (!(c.r > (M)0 && c.r < (M)1.0e30)) atomicOr(a.err, 1u);
+      if (a.write_fields) {
+        const float rf = (float)c.r, xf = (float)c.vx, yf = (float)c.vy, zf = (float)c.vz;
+        a.rho[i] = rf; a.ux[i] = xf; a.uy[i] = yf; a.uz[i] = zf;
+        if (dup) { a.rho[i + 1] = rf; a.ux[i + 1] = xf; a.uy[i + 1] = yf; a.uz[i + 1] = zf; }
+      } else if (a.mov && wall) {
+        a.rho[i] = (float)c.r;
+      }
+      const double s = sfrac_at(a, x, y, z);
+      S out[Q];
+      if (s != 0.0) {
+        const M sm = (M)s;
+        M px = (M)0, py = (M)0, pz = (M)0;
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+          const M fo = c.f[opp(q)];
+          const M d = c.gc[q] - fo;
+          px += (M)ex(q) * d; py += (M)ey(q) * d; pz += (M)ez(q) * d;
+          out[q] = to_store<M, S>(((M)1 - sm) * c.gc[q] + sm * fo);
+        }
+        Fx += (double)(sm * px); Fy += (double)(sm * py); Fz += (double)(sm * pz);
+      } else {
+#pragma unroll
+        for (int q = 0; q < Q; q++) out[q] = to_store<M, S>(c.gc[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < Q; q++) Gi[(IDX)a.dst[q]] = out[q];
+      if (dup) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) Gi[(IDX)a.dst[q] + 1] = out[q];
+      }
+    } else if (cat == CAT_EQ) {
+#pragma unroll
+      for (int q = 0; q < Q; q++) Gi[(IDX)a.dst[q]] = a.eq[q];
+      if (dup) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) Gi[(IDX)a.dst[q] + 1] = a.eq[q];
+      }
+      if (a.write_fields) {
+        a.ux[i] = a.u0f; a.uy[i] = 0.0f; a.uz[i] = 0.0f; a.rho[i] = 1.0f;
+        if (dup) { a.ux[i + 1] = a.u0f; a.uy[i + 1] = 0.0f; a.uz[i + 1] = 0.0f; a.rho[i + 1] = 1.0f; }
+      }
+    } else if (dup) {
+#pragma unroll
+      for (int q = 0; q < Q; q++) Gi[(IDX)a.dst[q] + 1] = Gi[(IDX)a.dst[q]];
+      if (a.write_fields) {
+        a.ux[i + 1] = a.ux[i]; a.uy[i + 1] = a.uy[i]; a.uz[i + 1] = a.uz[i]; a.rho[i + 1] = a.rho[i];
+      }
+    }
+  }
+  warp_force_partial(Fx, Fy, Fz, near_cell, a);
+}
+
+// ---- adjoint ------------------------------------------------------------------------
+
+template <class T>
+struct AdjArgs {
+  const T* Tn;     // adjoint of the next step: per consumer link, T[q*n + i]
+  T* Tc;           // this step's
+  double* ds;      // dJ/ds accumulated on the solid-fraction box
+  double wJ;       // weight of this step's force in J
+  int comp;        // force component of J
+};
+
+// Adjoint of the population stored at (q, location lx,ly,lz) after a step:
+// the sum of Tn over the links that pull it next step. loc_near: the
+// location is a computed near-wall cell whose neighbour bits are in m.
+template <class T, class S>
+__device__ __forceinline__ T adj_gather(const StepArgs<S>& a, const T* Tn, int q, int lx, int ly,
+                                        int lz, unsigned long long m) {
+  const int px = lx + ex(q), py = ly + ey(q), pz = lz + ez(q);
+  T v = (T)0;
+  if (px >= 0 && px < a.nx) v = Tn[(long long)q * a.n + px + (long long)a.nx * py + a.nxy * pz];
+  if ((m >> opp(q)) & 1ull)   // neighbour (px,py,pz) is solid: the location's own cell bounces it
+    v += Tn[(long long)opp(q) * a.n + lx + (long long)a.nx * ly + a.nxy * lz];
+  if (a.freeslip) {
+    const bool ym = py == 0 || py == a.ny - 1, zm = pz == 0 || pz == a.nz - 1;
+    if (ym || zm) {
+      const int sy = ym ? py : ly, sz = zm ? pz : lz;
+      if (!(a.flags[lx + (long long)a.nx * sy + a.nxy * sz] & FLAG_SOLID_MASK) && px >= 0 &&
+          px < a.nx) {
+        const int cy = ym ? ly : py, cz = zm ? lz : pz;
+        int qq = q;
+        if (ym) qq = mirror_y(qq);
+        if (zm) qq = mirror_z(qq);
+        v += Tn[(long long)qq * a.n + px + (long long)a.nx * cy + a.nxy * cz];
+      }
+    }
+  }
+  return v;
+}
+
+template <class S, class T>
+__global__ void __launch_bounds__(STEP_BX) k_adjoint(const __grid_constant__ StepArgs<S> a,
+                                                      const __grid_constant__ AdjArgs<T> j) {
+  const int x = blockIdx.x * STEP_BX + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z;
+  if (x >= a.nx) return;
+  const long long i = (long long)x + (long long)a.nx * y + a.nxy * z;
+  const uint8_t fl = a.flags[i];
+  const bool computed = x >= 1 && x <= a.nx - 2 && y >= 1 && y <= a.ny - 2 && z >= 1 &&
+                        z <= a.nz - 2 && !(fl & FLAG_SOLID_MASK);
+  T* Tci = j.Tc + i;
+  if (!computed) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) Tci[(long long)q * a.n] = (T)0;
+    return;
+  }
+  const unsigned long long m = (fl & FLAG_NEAR) ? a.nmask[i] : 0ull;
+  T gb[Q];
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    gb[q] = adj_gather<T>(a, j.Tn, q, x, y, z, m);
+    if (x == a.nx - 2) gb[q] += adj_gather<T>(a, j.Tn, q, x + 1, y, z, 0ull);   // outlet copy
+  }
+  // pulled populations (stationary walls) and the body links
+  CellFw<T> c;
+  const bool shell = a.freeslip && (y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2);
+  const unsigned sm = (unsigned)m, om = (unsigned)(m >> 32);
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    if ((sm >> q) & 1u) {
+      c.f[q] = (T)ld<T>(a.F[opp(q) * a.n + i]);
+    } else if (shell) {
+      int sy = y - ey(q), sz = z - ez(q), qq = q;
+      if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); }
+      if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); }
+      c.f[q] = (T)ld<T>(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);
+    } else {
+      c.f[q] = (T)ld<T>(a.F[a.src[q] + i]);
+    }
+  }
+  cell_fw<T>(a, c);
+  const double s = sfrac_at(a, x, y, z);
+  const T st = (T)s, wJ = (T)j.wJ;
+  T ab[Q], fb[Q];
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    const T cc = (T)(j.comp == 0 ? ex(q) : (j.comp == 1 ? ey(q) : ez(q)));
+    ab[q] = ((T)1 - st) * gb[q] + wJ * st * cc;
+    fb[q] = st * gb[opp(q)] + wJ * st * cc;
+    if ((om >> q) & 1u) fb[q] -= (T)2 * wJ * cc;
+  }
+  if (a.sfrac && x >= a.sb[0] && x < a.sb[3] && y >= a.sb[1] && y < a.sb[4] && z >= a.sb[2] &&
+      z < a.sb[5]) {
+    // dJ/ds = sum_q gb_q (f_opp(q) - gc_q) + wJ sum_q c_q (gc_q - f_opp(q))
+    T g1 = (T)0, g2 = (T)0;
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      const T cc = (T)(j.comp == 0 ? ex(q) : (j.comp == 1 ? ey(q) : ez(q)));
+      const T d = c.f[opp(q)] - c.gc[q];
+      g1 += gb[q] * d;
+      g2 -= cc * d;
+    }
+    j.ds[(x - a.sb[0]) + (long long)(a.sb[3] - a.sb[0]) *
+                             ((y - a.sb[1]) + (long long)(a.sb[4] - a.sb[1]) * (z - a.sb[2]))] +=
+        (double)(g1 + wJ * g2);
+  }
+  cell_vjp<T>(a, c, ab, fb);
+#pragma unroll
+  for (int q = 0; q < Q; q++) Tci[(long long)q * a.n] = fb[q];
+}
+
+}  // namespace wt

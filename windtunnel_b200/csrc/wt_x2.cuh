@@ -1,0 +1,409 @@
+// wt_x2.cuh — the fused step, two cells per thread, packed float32x2 collision.
+//
+// Same semantics and per-cell rules as k_step (wt_step.cuh). Thread t of a
+// block owns the adjacent cells x0 = 2*(blockIdx.x*X2_BX + t) and x0+1 of
+// row (y, z) = (blockIdx.y, blockIdx.z); nx must be even.
+//
+// Loads. Per direction q one aligned vector load (float2 / half2) fetches
+// the pair (x0, x0+1) of the source row (y - ey, z - ez). Directions with
+// ex = +1 need (x0-1, x0): x0-1 is the upper element of the previous lane's
+// pair, taken with a warp shuffle (lane 0 loads it); ex = -1 needs
+// (x0+1, x0+2), with x0+2 from the next lane (lane 31 loads it). No load is
+// misaligned and a warp's 19 loads cover exactly its 19 source row spans.
+//
+// Arithmetic. The two cells run the collision in lockstep with sm_100's
+// packed float32 instructions (add / sub / mul / fma .f32x2): cell x0 in the
+// .x lane of every float2, cell x0+1 in .y. The collision is that of
+// collide_fast (opposite pairs carried as half sums and half differences)
+// evaluated in the storage's scaled units: a half-storage lattice holds
+// 4096 * (f - w), and the collision is written so that this scale only
+// enters through r~ = 4096 + sum(f~) (moments, equilibrium, stress and the
+// TRT update are linear in f~, and the Smagorinsky term depends on
+// |Pi|/rho, which the scale leaves unchanged), so loads and stores carry no
+// scaling multiply. Reciprocals and square roots use the approximate
+// hardware instructions (relative error ~2^-22).
+//
+// Stores. The outputs of the pair go out as one packed vector store per
+// direction (one cvt.rn.f16x2.f32 per direction for half storage). Cells that
+// are not plain fluid follow k_step's rules per lane: bounce-back and
+// free-slip directions are re-gathered before the collision (patch_raw),
+// inlet / floor / edge-plane cells store the equilibrium, solid cells keep
+// their stale populations, and the outlet column x = nx-1 takes the values
+// that column nx-2 ends up holding.
+#pragma once
+
+#include "wt_vec.cuh"
+
+namespace wt {
+
+constexpr int X2_BX = 128;   // threads per block: 256 cells of one row
+
+// ---- packed float32 pairs: cell x0 in .x, cell x0+1 in .y --------------------------
+using f2 = float2;
+__device__ __forceinline__ f2 pk(float a) { return make_float2(a, a); }
+__device__ __forceinline__ f2 padd(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 pmul(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 pfma(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ f2 psub(f2 a, f2 b) {
+  unsigned long long ra, rb, rd;
+  memcpy(&ra, &a, 8);
+  memcpy(&rb, &b, 8);
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
+  f2 d;
+  memcpy(&d, &rd, 8);
+  return d;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ f2 prcp(f2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
+__device__ __forceinline__ f2 psqrt(f2 a) { return make_float2(sqrt_approx(a.x), sqrt_approx(a.y)); }
+
+template <int C>
+__device__ __forceinline__ float& lane_of(f2& v) {
+  if constexpr (C == 0) return v.x;
+  else return v.y;
+}
+
+// Storage in scaled units: raw(v) is the stored number as a float (the
+// deviation times SC), pack() rounds a pair of raw values to the storage.
+template <class S>
+struct X2;
+template <>
+struct X2<float> {
+  using V = float2;
+  static constexpr float SC = 1.0f;
+  __device__ __forceinline__ static float raw(float v) { return v; }
+  __device__ __forceinline__ static f2 unpack(V v) { return v; }
+  __device__ __forceinline__ static V pack(f2 g) { return g; }
+  __device__ __forceinline__ static float to_s(float v) { return v; }
+};
+template <>
+struct X2<__half> {
+  using V = __half2;
+  static constexpr float SC = (float)WT_F16_SCALE;
+  __device__ __forceinline__ static float raw(__half v) { return __half2float(v); }
+  __device__ __forceinline__ static f2 unpack(V v) { return __half22float2(v); }
+  __device__ __forceinline__ static V pack(f2 g) { return __float22half2_rn(g); }
+  __device__ __forceinline__ static __half to_s(float v) { return __float2half_rn(v); }
+};
+
+// Bounce-back / free-slip re-gather of lane C's cell i, in raw units
+// (js/lbm.js:334-368 for the bounce-back links; k_step's patch_special is
+// the same rule in deviation units). The momentum exchange accumulates in
+// raw units; the caller divides by SC.
+template <class S, int C>
+__device__ __forceinline__ void patch_raw(const StepArgs<S>& a, long long i, int x, int y, int z,
+                                          bool near_cell, bool shell, f2 (&f)[Q], double& Fx,
+                                          double& Fy, double& Fz) {
+  using T = X2<S>;
+  const unsigned long long m = near_cell ? a.nmask[i] : 0ull;
+  const unsigned sm = (unsigned)m, om = (unsigned)(m >> 32);
+  const float rho_sc = (a.mov && sm ? a.rho[i] : 1.0f) * T::SC;
+#define WT_PATCH_RAW(q)                                                                      \
+  if ((sm >> (q)) & 1u) {                                                                    \
+    const long long j = i - (ex(q) + (long long)ey(q) * a.nx + (long long)ez(q) * a.nxy);    \
+    const float fd = T::raw(a.F[opp(q) * a.n + i]);                                          \
+    float corr = 0.0f;                                                                       \
+    if (a.mov) {                                                                             \
+      const float cu = (float)ex(q) * a.uwx[j] + (float)ey(q) * a.uwy[j] +                   \
+                       (float)ez(q) * a.uwz[j];                                              \
+      if (cu != 0.0f) corr = 6.0f * (float)wq(q) * rho_sc * cu;                              \
+    }                                                                                        \
+    if ((om >> (q)) & 1u) {                                                                  \
+      const float d = 2.0f * fd + corr;                                                      \
+      Fx -= (double)(d * (float)ex(q));                                                      \
+      Fy -= (double)(d * (float)ey(q));                                                      \
+      Fz -= (double)(d * (float)ez(q));                                                      \
+    }                                                                                        \
+    lane_of<C>(f[q]) = fd + corr;                                                            \
+  } else if (shell) {                                                                        \
+    int sy = y - ey(q), sz = z - ez(q), qq = q;                                              \
+    bool refl = false;                                                                       \
+    if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); refl = true; }               \
+    if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); refl = true; }               \
+    if (refl)                                                                                \
+      lane_of<C>(f[q]) =                                                                     \
+          T::raw(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);           \
+  }
+  WT_PATCH_RAW(1) WT_PATCH_RAW(2) WT_PATCH_RAW(3) WT_PATCH_RAW(4) WT_PATCH_RAW(5)
+  WT_PATCH_RAW(6) WT_PATCH_RAW(7) WT_PATCH_RAW(8) WT_PATCH_RAW(9) WT_PATCH_RAW(10)
+  WT_PATCH_RAW(11) WT_PATCH_RAW(12) WT_PATCH_RAW(13) WT_PATCH_RAW(14) WT_PATCH_RAW(15)
+  WT_PATCH_RAW(16) WT_PATCH_RAW(17) WT_PATCH_RAW(18)
+#undef WT_PATCH_RAW
+}
+
+// Packed collision of two cells in raw (scaled) units: f -> g, with the
+// density r~ = SC * rho and the velocity of each lane. The mathematics is
+// that of js/lbm.js:377-460 (collide_fast's re-association).
+template <class S>
+__device__ __forceinline__ void collide_x2(const StepArgs<S>& a, f2 (&f)[Q], f2& r, f2& vx,
+                                           f2& vy, f2& vz) {
+  constexpr float SC = X2<S>::SC;
+  const f2 s1 = padd(f[1], f[2]), d1 = psub(f[1], f[2]);
+  const f2 s3 = padd(f[3], f[4]), d3 = psub(f[3], f[4]);
+  const f2 s5 = padd(f[5], f[6]), d5 = psub(f[5], f[6]);
+  const f2 s7 = padd(f[7], f[8]), d7 = psub(f[7], f[8]);
+  const f2 s9 = padd(f[9], f[10]), d9 = psub(f[9], f[10]);
+  const f2 s11 = padd(f[11], f[12]), d11 = psub(f[11], f[12]);
+  const f2 s13 = padd(f[13], f[14]), d13 = psub(f[13], f[14]);
+  const f2 s15 = padd(f[15], f[16]), d15 = psub(f[15], f[16]);
+  const f2 s17 = padd(f[17], f[18]), d17 = psub(f[17], f[18]);
+  const f2 dr = padd(padd(padd(f[0], s1), padd(s3, s5)),
+                     padd(padd(padd(s7, s9), padd(s11, s13)), padd(s15, s17)));
+  r = padd(pk(SC), dr);
+  const f2 inv = prcp(r);
+  const f2 jx = padd(padd(padd(d1, d7), padd(d9, d11)), d13);
+  const f2 jy = padd(psub(padd(d3, d7), d9), padd(d15, d17));
+  const f2 jz = padd(psub(padd(d5, d11), d13), psub(d15, d17));
+  vx = pmul(jx, inv);
+  vy = pmul(jy, inv);
+  vz = pmul(jz, inv);
+  const f2 usq = pfma(vz, vz, pfma(vy, vy, pmul(vx, vx)));
+  const f2 A = pfma(pmul(pk(-1.5f), r), usq, dr);   // dr - 1.5 r u^2 (scaled)
+  constexpr float WF = (float)(1.0 / 18), WE = (float)(1.0 / 36), W0 = (float)(1.0 / 3);
+  const f2 nwAF = pmul(pk(-WF), A), nwAE = pmul(pk(-WE), A);
+  const f2 nw45F = pmul(pk(-4.5f * WF), r), nw45E = pmul(pk(-4.5f * WE), r);
+  const f2 nw3F = pmul(pk(-3.0f * WF), r), nw3E = pmul(pk(-3.0f * WE), r);
+  const f2 c7 = padd(vx, vy), c9 = psub(vx, vy), c11 = padd(vx, vz), c13 = psub(vx, vz),
+           c15 = padd(vy, vz), c17 = psub(vy, vz);
+  const f2& c1 = vx;
+  const f2& c3 = vy;
+  const f2& c5 = vz;
+  // sp = (n_a + n_b)/2 = s/2 - w(A + 4.5 r c^2); sm = (n_a - n_b)/2 = d/2 - 3 w r c
+#define WT_PAIR2(k, C)                                                       \
+  const f2 sp##k = pfma(pk(0.5f), s##k, pfma(pmul(nw45##C, c##k), c##k, nwA##C)); \
+  const f2 sm##k = pfma(pk(0.5f), d##k, pmul(nw3##C, c##k));
+  WT_PAIR2(1, F) WT_PAIR2(3, F) WT_PAIR2(5, F) WT_PAIR2(7, E) WT_PAIR2(9, E) WT_PAIR2(11, E)
+  WT_PAIR2(13, E) WT_PAIR2(15, E) WT_PAIR2(17, E)
+#undef WT_PAIR2
+  f2 om = pk(a.omega0f), omm = pk(a.omm0f);
+  if (a.les) {
+    const f2 sxx = padd(padd(padd(sp1, sp7), padd(sp9, sp11)), sp13);
+    const f2 syy = padd(padd(padd(sp3, sp7), padd(sp9, sp15)), sp17);
+    const f2 szz = padd(padd(padd(sp5, sp11), padd(sp13, sp15)), sp17);
+    const f2 sxy = psub(sp7, sp9), sxz = psub(sp11, sp13), syz = psub(sp15, sp17);
+    const f2 off = pfma(syz, syz, pfma(sxz, sxz, pmul(sxy, sxy)));
+    const f2 qq = pfma(sxx, sxx, pfma(syy, syy, pfma(szz, szz, padd(off, off))));
+    // 72 cs2 sqrt(qq) / r: the scale of sqrt(qq~) and of r~ cancels
+    const f2 x = pmul(pmul(pk(a.les_cf), psqrt(qq)), inv);
+    const f2 te = pfma(pk(0.5f), psqrt(pfma(pk(a.tau0f), pk(a.tau0f), x)), pk(0.5f * a.tau0f));
+    om = prcp(te);
+    if (a.trt) {
+      const f2 t5 = psub(te, pk(0.5f));
+      omm = pmul(t5, prcp(pfma(pk(0.5f), t5, pk(a.lamf))));
+    } else {
+      omm = om;
+    }
+  }
+  const f2 nom = pmul(pk(-1.0f), om);
+  const f2 nomm = pmul(pk(-1.0f), omm);
+  f[0] = pfma(nom, psub(f[0], pmul(pk(W0), A)), f[0]);
+#define WT_OUT2(k, kb)                            \
+  {                                               \
+    const f2 base_a = pfma(nom, sp##k, f[k]);     \
+    const f2 base_b = pfma(nom, sp##k, f[kb]);    \
+    f[k] = pfma(nomm, sm##k, base_a);             \
+    f[kb] = pfma(omm, sm##k, base_b);             \
+  }
+  WT_OUT2(1, 2) WT_OUT2(3, 4) WT_OUT2(5, 6) WT_OUT2(7, 8) WT_OUT2(9, 10) WT_OUT2(11, 12)
+  WT_OUT2(13, 14) WT_OUT2(15, 16) WT_OUT2(17, 18)
+#undef WT_OUT2
+}
+
+// Source pair of direction q for the two cells of this thread, in raw units.
+template <class S, class IDX, int q>
+__device__ __forceinline__ f2 pull_pair(const S* Fp, long long srcq, int lane, bool active) {
+  using T = X2<S>;
+  using V = typename T::V;
+  const IDX base = (IDX)srcq + (IDX)ex(q);   // aligned pair (x0, x0+1) of the source row
+  V v;
+  if (active) v = *reinterpret_cast<const V*>(Fp + base);
+  else memset(&v, 0, sizeof(v));
+  if constexpr (ex(q) == 0) {
+    return T::unpack(v);
+  } else if constexpr (sizeof(S) == 4) {
+    if constexpr (ex(q) == 1) {
+      float prev = __shfl_up_sync(0xffffffffu, v.y, 1);
+      if (lane == 0 && active) prev = Fp[base - 1];
+      return make_float2(prev, v.x);
+    } else {
+      float nxt = __shfl_down_sync(0xffffffffu, v.x, 1);
+      if (lane == 31 && active) nxt = Fp[base + 2];
+      return make_float2(v.y, nxt);
+    }
+  } else {
+    unsigned w;
+    memcpy(&w, &v, 4);
+    if constexpr (ex(q) == 1) {
+      unsigned wp = __shfl_up_sync(0xffffffffu, w, 1);
+      if (lane == 0 && active) wp = (unsigned)__half_as_ushort(Fp[base - 1]) << 16;
+      const unsigned u = __byte_perm(wp, w, 0x5432);   // (prev.hi, this.lo)
+      V h;
+      memcpy(&h, &u, 4);
+      return T::unpack(h);
+    } else {
+      unsigned wn = __shfl_down_sync(0xffffffffu, w, 1);
+      if (lane == 31 && active) wn = (unsigned)__half_as_ushort(Fp[base + 2]);
+      const unsigned u = __byte_perm(w, wn, 0x5432);   // (this.hi, next.lo)
+      V h;
+      memcpy(&h, &u, 4);
+      return T::unpack(h);
+    }
+  }
+}
+
+template <class S, class IDX>
+__global__ void __launch_bounds__(X2_BX, 4) k_step_x2(const __grid_constant__ StepArgs<S> a) {
+  using T = X2<S>;
+  using V = typename T::V;
+  constexpr float SC = T::SC;
+  const int t = threadIdx.x;
+  const int lane = t & 31;
+  const int x0 = 2 * (blockIdx.x * X2_BX + t);
+  const int y = blockIdx.y, z = blockIdx.z;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const long long i0 = (long long)x0 + (long long)nx * y + a.nxy * z;
+  const bool active = x0 < nx;
+  const bool edge_row = z == 0 || z == nz - 1 || y == ny - 1;
+  double Fx = 0, Fy = 0, Fz = 0;
+  bool near_any = false;
+  S* Gi = a.G + i0;
+
+  if (edge_row) {
+    // ceiling / end planes: equilibrium for both cells (the outlet's copy of an
+    // equilibrium cell is the equilibrium)
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < Q; q++) {
+        V e;
+        const S eqs[2] = {a.eq[q], a.eq[q]};
+        memcpy(&e, eqs, sizeof(e));
+        *reinterpret_cast<V*>(Gi + (IDX)a.dst[q]) = e;
+      }
+      if (a.write_fields) {
+        a.ux[i0] = a.u0f; a.uy[i0] = 0.0f; a.uz[i0] = 0.0f; a.rho[i0] = 1.0f;
+        a.ux[i0 + 1] = a.u0f; a.uy[i0 + 1] = 0.0f; a.uz[i0 + 1] = 0.0f; a.rho[i0 + 1] = 1.0f;
+      }
+    }
+    pair_force_partial(Fx, Fy, Fz, near_any, a, x0 & ~31, y, z);
+    return;
+  }
+
+  uint8_t flA = 0, flB = 0;
+  if (active) {
+    flA = a.flags[i0];
+    flB = a.flags[i0 + 1];
+  }
+  const int catA = cell_category(a, x0, y, flA);
+  const int catB = (x0 + 1 == nx - 1) ? CAT_NONE : cell_category(a, x0 + 1, y, flB);
+  const bool fluidA = active && catA == CAT_FLUID, fluidB = active && catB == CAT_FLUID;
+
+  f2 f[Q];
+  f2 r = pk(SC), vx = pk(0.0f), vy = pk(0.0f), vz = pk(0.0f);
+  if (y == 0) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) f[q] = pk(0.0f);   // floor row: nothing is pulled
+  } else {
+    // interior row: vector pull of the 19 source rows (every lane takes part in the shuffles)
+    const S* Fp = a.F + i0;
+    f[0] = pull_pair<S, IDX, 0>(Fp, a.src[0], lane, active);
+    f[1] = pull_pair<S, IDX, 1>(Fp, a.src[1], lane, active);
+    f[2] = pull_pair<S, IDX, 2>(Fp, a.src[2], lane, active);
+    f[3] = pull_pair<S, IDX, 3>(Fp, a.src[3], lane, active);
+    f[4] = pull_pair<S, IDX, 4>(Fp, a.src[4], lane, active);
+    f[5] = pull_pair<S, IDX, 5>(Fp, a.src[5], lane, active);
+    f[6] = pull_pair<S, IDX, 6>(Fp, a.src[6], lane, active);
+    f[7] = pull_pair<S, IDX, 7>(Fp, a.src[7], lane, active);
+    f[8] = pull_pair<S, IDX, 8>(Fp, a.src[8], lane, active);
+    f[9] = pull_pair<S, IDX, 9>(Fp, a.src[9], lane, active);
+    f[10] = pull_pair<S, IDX, 10>(Fp, a.src[10], lane, active);
+    f[11] = pull_pair<S, IDX, 11>(Fp, a.src[11], lane, active);
+    f[12] = pull_pair<S, IDX, 12>(Fp, a.src[12], lane, active);
+    f[13] = pull_pair<S, IDX, 13>(Fp, a.src[13], lane, active);
+    f[14] = pull_pair<S, IDX, 14>(Fp, a.src[14], lane, active);
+    f[15] = pull_pair<S, IDX, 15>(Fp, a.src[15], lane, active);
+    f[16] = pull_pair<S, IDX, 16>(Fp, a.src[16], lane, active);
+    f[17] = pull_pair<S, IDX, 17>(Fp, a.src[17], lane, active);
+    f[18] = pull_pair<S, IDX, 18>(Fp, a.src[18], lane, active);
+    if (fluidA || fluidB) {
+      const bool shell = a.freeslip && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
+      const bool nearA = fluidA && (flA & FLAG_NEAR) != 0;
+      const bool nearB = fluidB && (flB & FLAG_NEAR) != 0;
+      near_any = nearA || nearB;
+      if (fluidA && (nearA || shell)) patch_raw<S, 0>(a, i0, x0, y, z, nearA, shell, f, Fx, Fy, Fz);
+      if (fluidB && (nearB || shell))
+        patch_raw<S, 1>(a, i0 + 1, x0 + 1, y, z, nearB, shell, f, Fx, Fy, Fz);
+      collide_x2<S>(a, f, r, vx, vy, vz);
+      if ((fluidA && !(r.x > 0.0f && r.x < 3.0e38f)) || (fluidB && !(r.y > 0.0f && r.y < 3.0e38f)))
+        atomicOr(a.err, 1u);
+      if (a.mov && !a.write_fields) {
+        if (nearA) a.rho[i0] = r.x * (1.0f / SC);
+        if (nearB) a.rho[i0 + 1] = r.y * (1.0f / SC);
+      }
+    }
+  }
+
+  if (active) {
+    // lane selection: fluid -> collided, equilibrium -> eq, solid -> keep,
+    // outlet (cell B at x = nx-1) -> whatever cell A ends up holding
+    const bool eqA = catA == CAT_EQ, eqB = catB == CAT_EQ;
+    const bool keepA = catA == CAT_KEEP;
+    const bool outB = catB == CAT_NONE;
+    const bool storeA = !keepA, storeB = catB != CAT_KEEP;
+    if (storeA && storeB && !eqA && !eqB && !outB) {
+#pragma unroll
+      for (int q = 0; q < Q; q++) *reinterpret_cast<V*>(Gi + (IDX)a.dst[q]) = T::pack(f[q]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < Q; q++) {
+        S sa, sb;
+        const V pv = T::pack(f[q]);
+        S two[2];
+        memcpy(two, &pv, sizeof(two));
+        sa = eqA ? a.eq[q] : two[0];
+        sb = eqB ? a.eq[q] : two[1];
+        if (outB) sb = keepA ? Gi[(IDX)a.dst[q]] : sa;
+        if (storeA && storeB) {
+          const S pair[2] = {sa, sb};
+          V o;
+          memcpy(&o, pair, sizeof(o));
+          *reinterpret_cast<V*>(Gi + (IDX)a.dst[q]) = o;
+        } else if (storeA) {
+          Gi[(IDX)a.dst[q]] = sa;
+        } else if (storeB) {
+          Gi[(IDX)a.dst[q] + 1] = sb;
+        }
+      }
+    }
+    if (a.write_fields) {
+      float ra = 1.0f, xa = a.u0f, ya = 0.0f, za = 0.0f;
+      if (fluidA) { ra = r.x * (1.0f / SC); xa = vx.x; ya = vy.x; za = vz.x; }
+      if (keepA) { ra = a.rho[i0]; xa = a.ux[i0]; ya = a.uy[i0]; za = a.uz[i0]; }
+      else { a.rho[i0] = ra; a.ux[i0] = xa; a.uy[i0] = ya; a.uz[i0] = za; }
+      if (outB) {
+        a.rho[i0 + 1] = ra; a.ux[i0 + 1] = xa; a.uy[i0 + 1] = ya; a.uz[i0 + 1] = za;
+      } else if (fluidB) {
+        a.rho[i0 + 1] = r.y * (1.0f / SC); a.ux[i0 + 1] = vx.y; a.uy[i0 + 1] = vy.y;
+        a.uz[i0 + 1] = vz.y;
+      } else if (eqB) {
+        a.rho[i0 + 1] = 1.0f; a.ux[i0 + 1] = a.u0f; a.uy[i0 + 1] = 0.0f; a.uz[i0 + 1] = 0.0f;
+      }
+    }
+  }
+  constexpr double inv_sc = 1.0 / (double)SC;   // a power of two: exact
+  pair_force_partial(Fx * inv_sc, Fy * inv_sc, Fz * inv_sc, near_any, a, x0 & ~31, y, z);
+}
+
+inline dim3 x2_grid(int nx, int ny, int nz) {
+  return dim3((unsigned)((nx + 2 * X2_BX - 1) / (2 * X2_BX)), (unsigned)ny, (unsigned)nz);
+}
+
+}  // namespace wt

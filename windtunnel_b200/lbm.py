@@ -32,7 +32,8 @@ STORAGE = {"f32": W.WT_STORE_F32, "f16dev": W.WT_STORE_F16DEV, "f64": W.WT_STORE
 MATH = {"fast": W.WT_MATH_FAST, "exact": W.WT_MATH_EXACT}
 SIDE = {"eq": W.WT_SIDE_EQ, "freeslip": W.WT_SIDE_FREESLIP}
 KERNEL = {"auto": W.WT_KERNEL_AUTO, "direct": W.WT_KERNEL_DIRECT, "staged": W.WT_KERNEL_STAGED,
-          "vector": W.WT_KERNEL_VECTOR, "pipe": W.WT_KERNEL_PIPE}
+          "vector": W.WT_KERNEL_VECTOR, "pipe": W.WT_KERNEL_PIPE, "x2": W.WT_KERNEL_X2,
+          "tma": W.WT_KERNEL_TMA}
 _STORE_DTYPE = {W.WT_STORE_F32: np.float32, W.WT_STORE_F16DEV: np.float16,
                 W.WT_STORE_F64: np.float64}
 
@@ -383,6 +384,31 @@ class LBM:
     @property
     def g(self) -> np.ndarray:
         return self.populations("g")
+
+    # ---- partial bounce-back and its adjoint (no reference counterpart) ------------------
+    def set_solid_fraction(self, box, s) -> None:
+        """Solid fraction on the half-open box (x0, y0, z0, x1, y1, z1); s is indexed
+        [z][y][x] over the box. box=None clears the field."""
+        if box is None:
+            self._call(lib().wt_set_solid_fraction, None, None)
+            self._sbox = None
+            return
+        b = (C.c_int * 6)(*[int(v) for v in box])
+        a = np.ascontiguousarray(s, np.float64).ravel()
+        self._call(lib().wt_set_solid_fraction, b, _dptr(a))
+        self._sbox = tuple(int(v) for v in box)
+
+    def adjoint(self, nsteps: int, window: int, component: int = 0, checkpoint: int = 0):
+        """(J, dJ/ds as [z][y][x] over the box, stats): J is the mean force component
+        over the last `window` of `nsteps` steps from the current state."""
+        x0, y0, z0, x1, y1, z1 = self._sbox
+        g = np.empty((z1 - z0, y1 - y0, x1 - x0), np.float64)
+        cfg = W.wt_adj_cfg(int(nsteps), int(window), int(component), int(checkpoint))
+        st = W.wt_adj_stats()
+        self._call(lib().wt_adjoint, C.byref(cfg), _dptr(g), C.byref(st))
+        self._fields_at = -1
+        stats = {k: getattr(st, k) for k, _ in W.wt_adj_stats._fields_}
+        return st.J, g, stats
 
     # ---- checkpoint ------------------------------------------------------------------------
     def get_state(self) -> bytes:
