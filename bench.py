@@ -4,7 +4,8 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl wt|reference]
 
 Workload (default): the 256x128x128 channel with a 15-degree-yawed
-superellipsoid hull (80x30x24 cells), u0 = 0.06, Re = 2000 on the length
+superellipsoid hull (80x30x24 cells, 20000 triangles with a seeded bump
+field, voxelised on the GPU by Voxel.build), u0 = 0.06, Re = 2000 on the length
 (tau = 0.5072), TRT Lambda = 3/16, Smagorinsky Cs = 0.1, free-slip side
 planes, seeded +-1e-4 velocity noise. A "step" is one lattice time step
 over all 4,194,304 cells; MLUPS counts every cell (the reference's
@@ -71,10 +72,23 @@ WORKLOADS = {
 
 
 # ---------------------------------------------------------------------------- set-up
+_GRIDS = {}
+
+
 def body_inputs(wl):
-    from windtunnel_b200.bodies import body_box, body_matrix, superellipsoid_grid
+    """The benchmark body: a seeded 20000-triangle superellipsoid hull with a
+    radial bump field, oriented and length-normalised (Shapes.orient), voxelised
+    on the GPU with Voxel.build at `res` cells along its length, placed at
+    scale / yaw / pos by the device lookup."""
+    from windtunnel_b200.bodies import body_box, body_matrix
+    from windtunnel_b200.mesh import hull_mesh, orient, voxel_build
     b = wl["body"]
-    vg = superellipsoid_grid(b["semi"], b["exponent"], b["res"])
+    key = (b["semi"], b["exponent"], b["res"])
+    if key not in _GRIDS:
+        tris = hull_mesh(semi=b["semi"], exponent=b["exponent"], seed=wl["seed"])
+        orient(tris, 0, 1)
+        _GRIDS[key] = voxel_build(tris, b["res"])
+    vg = _GRIDS[key]
     M = body_matrix(math.radians(b["yaw_deg"]), 0.0)
     P = [0.36 * wl["nx"], 0.5 * wl["ny"], 0.5 * wl["nz"]]
     box = body_box(M, vg.ext, b["scale"], P)
@@ -311,8 +325,8 @@ def accuracy_study(wl, long_steps: int = 20000) -> dict:
                       "16-block blocking SEM (js/main.js:163-191)"}
     res = {}
     forms = (("f64", "f64", "exact", None), ("f32", "f32", "fast", None),
-             ("f16dev", "f16dev", "fast", "stochastic"),
-             ("f16dev_nearest", "f16dev", "fast", "nearest"))
+             ("f16dev", "f16dev", "fast", "nearest"),
+             ("f16dev_stochastic", "f16dev", "fast", "stochastic"))
     for name, storage, mm, rounding in forms:
         sim = setup_gpu(wl, storage, mm)
         if rounding:
@@ -342,6 +356,135 @@ def accuracy_study(wl, long_steps: int = 20000) -> dict:
             e["dcd_long_sigma"] = abs(e["cd_long"] - ref["cd_long"]) / math.hypot(
                 e["cd_long_sem"], ref["cd_long_sem"])
     out.update(res)
+    return out
+
+
+# ---------------------------------------------------------------------------- adjoint
+ADJOINT_WORKLOADS = {
+    "design128": dict(
+        name="128x64x64 channel, 32^3 partial-bounce-back design box at (40,32,32), Re=100",
+        nx=128, ny=64, nz=64, u0=0.05, tau=0.53, csm=0.1, lam=3 / 16, les=True,
+        side_bc="freeslip", box=(24, 16, 16, 56, 48, 48), centre=(40.0, 32.0, 32.0),
+        radius=10.0, width=1.5, noise=0.05, seed=1234, amp=1e-4, steps=1500, window=500,
+        checkpoint=50, storage="f32", fd_cells=16, fd_eps=1e-3),
+    "design384": dict(
+        name="384x160x160 channel, 64^3 partial-bounce-back design box at (120,80,80), Re=1000",
+        nx=384, ny=160, nz=160, u0=0.05, tau=0.506, csm=0.1, lam=3 / 16, les=True,
+        side_bc="freeslip", box=(88, 48, 48, 152, 112, 112), centre=(120.0, 80.0, 80.0),
+        radius=20.0, width=1.5, noise=0.05, seed=1234, amp=1e-4, steps=4000, window=1000,
+        checkpoint=0, storage="f16dev", fd_cells=0, fd_eps=0.0),
+}
+
+
+def design_field(aw) -> "np.ndarray":
+    """s = (1 - tanh((|x - c| - r) / w)) / 2 + U(-noise, noise), clipped to [0, 1]."""
+    import numpy as np
+    x0, y0, z0, x1, y1, z1 = aw["box"]
+    zz, yy, xx = np.meshgrid(np.arange(z0, z1) + 0.5, np.arange(y0, y1) + 0.5,
+                             np.arange(x0, x1) + 0.5, indexing="ij")
+    cx, cy, cz = aw["centre"]
+    r = np.sqrt((xx - cx) ** 2 + (yy - cy) ** 2 + (zz - cz) ** 2)
+    rng = np.random.default_rng(aw["seed"])
+    s = 0.5 * (1 - np.tanh((r - aw["radius"]) / aw["width"]))
+    s = s + rng.uniform(-aw["noise"], aw["noise"], r.shape)
+    return np.clip(s, 0.0, 1.0)
+
+
+def design_lattice(aw, storage, math_mode="fast", s=None):
+    from windtunnel_b200 import LBM
+    sim = LBM(aw["nx"], aw["ny"], aw["nz"], storage=storage, math=math_mode,
+              side_bc=aw["side_bc"])
+    sim.set_params(u0=aw["u0"], tau=aw["tau"], csm=aw["csm"], les=int(aw["les"]),
+                   **{"lambda": aw["lam"]})
+    sim.init_eq_noise(aw["seed"], aw["amp"])
+    sim.set_solid_fraction(aw["box"], design_field(aw) if s is None else s)
+    return sim
+
+
+def adjoint_study(aw) -> dict:
+    """Adjoint gradient time over forward time on a design-box workload, with
+    gradient checks: FP64 central differences (when fd_cells > 0), the FP64
+    adjoint, and the FP32-storage adjoint against the workload's storage form."""
+    import numpy as np
+    import torch
+    N, W, C = aw["steps"], aw["window"], aw["checkpoint"]
+    out = {"workload": aw["name"], "steps": N, "window": W, "storage": aw["storage"],
+           "objective": "mean drag (Fx) over the last window steps"}
+    # plain forward of the same lattice (events on the library stream)
+    sim = design_lattice(aw, aw["storage"])
+    sim.step_forces(3)
+    sim.close()
+    sim = design_lattice(aw, aw["storage"])
+    st = torch.cuda.ExternalStream(sim.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    F = sim.step_forces(N)
+    e1.record(st)
+    e1.synchronize()
+    t_fwd = e0.elapsed_time(e1)
+    J_fwd = float(F[-W:, 0].mean())
+    sim.close()
+    # gradient: forward sweep with checkpoints + recompute + adjoint
+    sim = design_lattice(aw, aw["storage"])
+    free0 = torch.cuda.mem_get_info()[0]
+    e0.record(st := torch.cuda.ExternalStream(sim.stream))
+    J, g, stats = sim.adjoint(N, W, 0, C)
+    e1.record(st)
+    e1.synchronize()
+    t_adj = e0.elapsed_time(e1)
+    sim.close()
+    out.update(forward_ms=round(t_fwd, 2), gradient_ms=round(t_adj, 2),
+               ratio=round(t_adj / t_fwd, 3),
+               backward_only_ratio=round(stats["backward_ms"] / t_fwd, 3),
+               checkpoint_interval=stats["segment"], checkpoints=stats["checkpoints"],
+               adjoint_device_bytes=stats["device_bytes"],
+               device_free_before_bytes=int(free0), J=J, J_plain_forward=J_fwd)
+    # the same gradient with float32 storage (for the half-storage forward) or float64
+    ref_storage = "f32" if aw["storage"] == "f16dev" else "f64"
+    sim = design_lattice(aw, ref_storage, "exact" if ref_storage == "f64" else "fast")
+    Jr, gr, _ = sim.adjoint(N, W, 0, C)
+    sim.close()
+    cos = float((g * gr).sum() / (np.linalg.norm(g) * np.linalg.norm(gr)))
+    out[f"vs_{ref_storage}_adjoint"] = {
+        "cosine": cos, "rel_l2": float(np.linalg.norm(g - gr) / np.linalg.norm(gr)),
+        "J_rel": abs(J - Jr) / abs(Jr)}
+    if aw["fd_cells"]:
+        rng = np.random.default_rng(aw["seed"] + 1)
+        shape = g.shape
+        s0 = design_field(aw)
+        eps = aw["fd_eps"]
+        rows = []
+        for _ in range(aw["fd_cells"]):
+            idx = tuple(int(rng.integers(0, n)) for n in shape)
+            js = []
+            for sgn in (1, -1):
+                sv = s0.copy()
+                sv[idx] += sgn * eps
+                fsim = design_lattice(aw, "f64", "exact", s=sv)
+                js.append(float(fsim.step_forces(N)[-W:, 0].mean()))
+                fsim.close()
+            fd = (js[0] - js[1]) / (2 * eps)
+            rows.append((g[idx], gr[idx], fd))
+        rows = np.array(rows)
+        scale = np.abs(rows[:, 2]).max()
+        out["fd_check"] = {
+            "cells": aw["fd_cells"], "eps": eps, "fd": "central, float64 storage + arithmetic",
+            "max_rel_err_adjoint": float(np.max(np.abs(rows[:, 0] - rows[:, 2]) /
+                                                np.maximum(np.abs(rows[:, 2]), 1e-300))),
+            "max_err_over_max_fd_adjoint": float(np.max(np.abs(rows[:, 0] - rows[:, 2])) / scale),
+            "max_rel_err_f64_adjoint": float(np.max(np.abs(rows[:, 1] - rows[:, 2]) /
+                                                    np.maximum(np.abs(rows[:, 2]), 1e-300))),
+            "max_err_over_max_fd_f64_adjoint": float(np.max(np.abs(rows[:, 1] - rows[:, 2])) /
+                                                     scale)}
+    else:
+        # drag of the storage form against a float64 run of the same case
+        sim = design_lattice(aw, "f64", "exact")
+        F64 = sim.step_forces(N)
+        sim.close()
+        J64 = float(F64[-W:, 0].mean())
+        # Cd is J over the same dynamic pressure and area: the relative errors coincide
+        out["cd_rel_err_vs_f64"] = abs(J_fwd - J64) / abs(J64)
     return out
 
 
@@ -433,6 +576,10 @@ def run_wt(args) -> None:
     if args.accuracy and dist.rank == 0:
         line["accuracy"] = accuracy_study(wl)
         line["accuracy_steady"] = accuracy_study(WORKLOADS["sphere128"], long_steps=0)
+    if args.adjoint and dist.rank == 0:
+        line["adjoint"] = adjoint_study(ADJOINT_WORKLOADS["design128"])
+        if args.adjoint_scale:
+            line["adjoint_scale"] = adjoint_study(ADJOINT_WORKLOADS["design384"])
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl)
     dist.barrier()
@@ -496,6 +643,8 @@ def main() -> None:
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="channel256")
     ap.add_argument("--no-accuracy", dest="accuracy", action="store_false")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
+    ap.add_argument("--no-adjoint-scale", dest="adjoint_scale", action="store_false")
     ap.add_argument("--reference-budget", type=float, default=90.0,
                     help="seconds of timed CPU work for --impl reference")
     args = ap.parse_args()

@@ -72,7 +72,8 @@ enum {
 
 /* Which step kernel runs. */
 enum {
-  WT_KERNEL_AUTO = 0,    /* the kernel measured fastest on B200 for the form: direct */
+  WT_KERNEL_AUTO = 0,    /* the kernel measured fastest on B200 for the form: LEAN for half
+                            storage (when it can run), DIRECT otherwise */
   WT_KERNEL_DIRECT = 1,  /* one thread per cell, populations gathered straight from HBM */
   WT_KERNEL_STAGED = 2,  /* persistent CTAs staging the 19 pull rows with bulk copies (TMA);
                             needs nx to be a multiple of 16 bytes / element size */
@@ -83,9 +84,13 @@ enum {
   WT_KERNEL_X2 = 5,      /* two cells per thread with paired vector loads / stores and the
                             collision of both cells in packed float32x2 instructions; float32
                             collision, nx even, nearest rounding for half storage */
-  WT_KERNEL_TMA = 6      /* persistent CTAs moving 128x4-cell tiles of all 19 directions through
+  WT_KERNEL_TMA = 6,     /* persistent CTAs moving 512-cell tiles of all 19 directions through
                             shared memory with tensor-map TMA loads and stores, packed float32x2
                             collision; float32 collision, nx a multiple of 16 bytes / element,
+                            nearest rounding for half storage */
+  WT_KERNEL_LEAN = 7     /* one thread per cell, 32-bit byte offsets from one pointer per cell,
+                            the collision in storage units with approximate reciprocal / square
+                            root; float32 collision, buffers under 2 GiB, stationary walls,
                             nearest rounding for half storage */
 };
 
@@ -209,7 +214,8 @@ int wt_step(wt_lattice* h, int nsteps, double* forces);
  * per-step forces and the error word in one fixed device array of about
  * 3.2 MB instead (16384 wall segments x 8 steps of partials, 4096 steps of
  * forces), located once per device with cudaGetSymbolAddress.
- * Same results as wt_step with the direct kernel (kernel AUTO or DIRECT).
+ * Same results as wt_step: it runs the kernel wt_step picks for kernel
+ * AUTO, DIRECT or LEAN (the one-cell-per-thread kernels).
  * Limits: nsteps in 0..4096 (else WT_ERR_ARG); a body with more than 16384
  * 32-cell wall segments gives WT_ERR_UNSUPPORTED; the lattice's device must
  * be the current device (else WT_ERR_STATE). The first call on a device sets
@@ -255,6 +261,39 @@ typedef struct wt_adj_stats {
  * float64 storage or WT_MATH_EXACT, float32 otherwise. Stationary walls only
  * (WT_ERR_UNSUPPORTED with moving walls); WT_ERR_STATE without a field. */
 int wt_adjoint(wt_lattice* h, const wt_adj_cfg* cfg, double* dJds, wt_adj_stats* stats);
+
+/* Voxel.build (js/voxel.js:48-102): a triangle soup in body space becomes a
+ * body-space occupancy grid for wt_voxelize_grid. The fields follow the
+ * returned object of js/voxel.js:89-101. */
+typedef struct wt_voxel_info {
+  int32_t nx, ny, nz;   /* grid dims (2 cells of padding each side) */
+  int32_t reserved;
+  int64_t tris;         /* stats.tris */
+  double cell, inv;     /* cell size and 1 / cell */
+  double min[3];        /* grid min corner */
+  double ext[3];        /* half extents of the mesh bounds */
+  double centre[3];     /* centre of the mesh bounds */
+  double bbox[6];       /* mesh bounds x0, y0, z0, x1, y1, z1 */
+  int64_t solid;        /* stats.solid: occupied cells */
+  double openness;      /* stats.openness: cells where the three parity votes disagree / solid */
+} wt_voxel_info;
+
+/* The grid dims, cell size and bounds for `res` cells along the longest
+ * axis (js/voxel.js:48-71), without building: tris holds 9*ntri floats.
+ * Errors (WT_ERR_ARG, message in wt_voxel_last_error): no triangles, a
+ * degenerate mesh, a grid of more than 40e6 cells (js/voxel.js:51, :56, :71). */
+int wt_voxel_dims(const float* tris, int64_t ntri, int res, wt_voxel_info* info);
+
+/* Voxel.build(P, res) on the current CUDA device — js/voxel.js:48-232: the
+ * surface shell OR'd with a two-of-three vote of ray-parity fills along x, y
+ * and z, in float64 with the reference's operation order (bit-identical to
+ * the reference). grid (grid_len = nx*ny*nz bytes, index x + nx*(y + ny*z))
+ * receives 1 for solid cells. Allocates and frees its own device buffers. */
+int wt_voxel_build(const float* tris, int64_t ntri, int res, uint8_t* grid, size_t grid_len,
+                   wt_voxel_info* info);
+
+/* Message of the last failed wt_voxel_* call on this thread. */
+const char* wt_voxel_last_error(void);
 
 /* LBM.force — js/lbm.js:113, :289: the force of the last step. */
 int wt_get_force(const wt_lattice* h, double out[3]);

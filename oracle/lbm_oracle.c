@@ -286,6 +286,207 @@ static void or_collide_vjp(const wt_params* p, const or_cellfw* c, const double 
     fb[q] += drb + (OR_EX[q] * jxb + OR_EY[q] * jyb + OR_EZ[q] * jzb);
 }
 
+/* ---- Voxel.build, js/voxel.js:32-232 ------------------------------------------
+ * Triangle soup (float32, 9 per triangle, body space) -> body-space occupancy
+ * grid: surface shell rasterisation OR'd with a 2-of-3 vote of ray-parity
+ * fills along x, y and z. float64 arithmetic in the reference's operation
+ * order (JavaScript numbers). */
+typedef struct {
+  int nx, ny, nz, tris;
+  double cell, inv, min[3], ext[3], centre[3], bbox[6];
+  long solid;
+  double openness;
+} or_voxel_info;
+
+/* js/voxel.js:32-42 and :48-71: bounds, cell size, padded dims, min corner.
+ * Returns 0, -1 (no triangles), -2 (degenerate), -3 (grid too large). */
+int or_voxel_dims(const float* P, long ntri, int res, or_voxel_info* vi) {
+  if (res <= 0) res = 96;
+  if (ntri <= 0) return -1;
+  double x0 = INFINITY, y0 = INFINITY, z0 = INFINITY, x1 = -INFINITY, y1 = -INFINITY, z1 = -INFINITY;
+  for (long i = 0; i < 9 * ntri; i += 3) {
+    const double x = P[i], y = P[i + 1], z = P[i + 2];
+    if (x < x0) x0 = x;
+    if (x > x1) x1 = x;
+    if (y < y0) y0 = y;
+    if (y > y1) y1 = y;
+    if (z < z0) z0 = z;
+    if (z > z1) z1 = z;
+  }
+  const double sx = x1 - x0, sy = y1 - y0, sz = z1 - z0;
+  const double span = fmax(fmax(sx, sy), sz);
+  if (!(span > 0)) return -2;
+  const double cell = span / res;
+  const int PAD = 2;
+  const double dx = fmax(3, ceil(sx / cell) + 2 * PAD), dy = fmax(3, ceil(sy / cell) + 2 * PAD),
+               dz = fmax(3, ceil(sz / cell) + 2 * PAD);
+  if (dx * dy * dz > 40e6) return -3;
+  vi->nx = (int)dx; vi->ny = (int)dy; vi->nz = (int)dz;
+  vi->tris = (int)ntri;
+  vi->cell = cell;
+  vi->inv = 1 / cell;
+  vi->min[0] = x0 - (vi->nx * cell - sx) * 0.5;
+  vi->min[1] = y0 - (vi->ny * cell - sy) * 0.5;
+  vi->min[2] = z0 - (vi->nz * cell - sz) * 0.5;
+  vi->ext[0] = sx * 0.5; vi->ext[1] = sy * 0.5; vi->ext[2] = sz * 0.5;
+  vi->centre[0] = (x0 + x1) * 0.5; vi->centre[1] = (y0 + y1) * 0.5; vi->centre[2] = (z0 + z1) * 0.5;
+  vi->bbox[0] = x0; vi->bbox[1] = y0; vi->bbox[2] = z0;
+  vi->bbox[3] = x1; vi->bbox[4] = y1; vi->bbox[5] = z1;
+  vi->solid = 0;
+  vi->openness = 0;
+  return 0;
+}
+
+static int or_cmp_double(const void* a, const void* b) {
+  const double x = *(const double*)a, y = *(const double*)b;
+  return (x > y) - (x < y);
+}
+
+/* js/voxel.js:105-137: mark every cell the surface passes through. */
+static void or_raster_surface(const float* P, long ntri, uint8_t* shell, const or_voxel_info* vi) {
+  const int nx = vi->nx, ny = vi->ny, nz = vi->nz;
+  const double inv = 1 / vi->cell;
+  for (long t = 0; t < ntri; t++) {
+    const float* o = P + 9 * t;
+    const double ax = o[0], ay = o[1], az = o[2], bx = o[3], by = o[4], bz = o[5];
+    const double cx = o[6], cy = o[7], cz = o[8];
+    const double e1 = fmax(fmax(fabs(bx - ax), fabs(by - ay)), fabs(bz - az));
+    const double e2 = fmax(fmax(fabs(cx - ax), fabs(cy - ay)), fabs(cz - az));
+    double n1 = ceil(e1 * inv * 2) + 1, n2 = ceil(e2 * inv * 2) + 1;
+    if (n1 * n2 > 4096) {
+      const double k = sqrt(4096 / (n1 * n2));
+      n1 = fmax(2, (double)or_toint32(n1 * k));
+      n2 = fmax(2, (double)or_toint32(n2 * k));
+    }
+    for (double i = 0; i <= n1; i++) {
+      const double u = i / n1;
+      const double jmax = ceil((1 - u) * n2);
+      for (double j = 0; j <= jmax; j++) {
+        const double v = fmin(j / n2, 1 - u);
+        const double x = ax + (bx - ax) * u + (cx - ax) * v;
+        const double y = ay + (by - ay) * u + (cy - ay) * v;
+        const double z = az + (bz - az) * u + (cz - az) * v;
+        const int32_t gx = or_toint32((x - vi->min[0]) * inv);
+        const int32_t gy = or_toint32((y - vi->min[1]) * inv);
+        const int32_t gz = or_toint32((z - vi->min[2]) * inv);
+        if (gx < 0 || gy < 0 || gz < 0 || gx >= nx || gy >= ny || gz >= nz) continue;
+        shell[gx + (long)nx * (gy + (long)ny * gz)] = 1;
+      }
+    }
+  }
+}
+
+/* js/voxel.js:144-232: ray parity along `axis`, one ray per column. */
+static int or_parity_fill(const float* P, long ntri, uint8_t* votes, const or_voxel_info* vi,
+                          int axis) {
+  const int dim[3] = {vi->nx, vi->ny, vi->nz};
+  const int A = axis, B = (axis + 1) % 3, C = (axis + 2) % 3;
+  const int nA = dim[A], nB = dim[B], nC = dim[C];
+  const double cell = vi->cell;
+  const double minA = vi->min[A], minB = vi->min[B], minC = vi->min[C];
+  const double spanB = nB * cell, spanC = nC * cell;
+  const int nbB = nB < 48 ? nB : 48, nbC = nC < 48 ? nC : 48;
+  const double kB = nbB / spanB, kC = nbC / spanC;
+  const int nb = nbB * nbC;
+  int* count = (int*)calloc((size_t)nb + 1, sizeof(int));
+  int* lo = (int*)malloc(sizeof(int) * 2 * (size_t)ntri);
+  int* hi = (int*)malloc(sizeof(int) * 2 * (size_t)ntri);
+  double* hits = (double*)malloc(sizeof(double) * 512);
+  if (!count || !lo || !hi || !hits) { free(count); free(lo); free(hi); free(hits); return -1; }
+  for (long t = 0; t < ntri; t++) {
+    const float* o = P + 9 * t;
+    const double b0 = o[B], b1 = o[3 + B], b2 = o[6 + B];
+    const double c0 = o[C], c1 = o[3 + C], c2 = o[6 + C];
+    double bl = floor((fmin(fmin(b0, b1), b2) - minB) * kB);
+    double bh = floor((fmax(fmax(b0, b1), b2) - minB) * kB);
+    double cl = floor((fmin(fmin(c0, c1), c2) - minC) * kC);
+    double ch = floor((fmax(fmax(c0, c1), c2) - minC) * kC);
+    bl = bl < 0 ? 0 : bl; bh = bh >= nbB ? nbB - 1 : bh;
+    cl = cl < 0 ? 0 : cl; ch = ch >= nbC ? nbC - 1 : ch;
+    lo[2 * t] = (int)bl; hi[2 * t] = (int)bh; lo[2 * t + 1] = (int)cl; hi[2 * t + 1] = (int)ch;
+    if (bl > bh || cl > ch) continue;
+    for (int cc = (int)cl; cc <= (int)ch; cc++)
+      for (int bb = (int)bl; bb <= (int)bh; bb++) count[bb + nbB * cc + 1]++;
+  }
+  for (int i = 0; i < nb; i++) count[i + 1] += count[i];
+  int* items = (int*)malloc(sizeof(int) * ((size_t)count[nb] + 1));
+  int* cursor = (int*)malloc(sizeof(int) * (size_t)nb);
+  if (!items || !cursor) { free(count); free(lo); free(hi); free(hits); free(items); free(cursor); return -1; }
+  memcpy(cursor, count, sizeof(int) * (size_t)nb);
+  for (long t = 0; t < ntri; t++) {
+    const int bl = lo[2 * t], bh = hi[2 * t], cl = lo[2 * t + 1], ch = hi[2 * t + 1];
+    if (bl > bh || cl > ch) continue;
+    for (int cc = cl; cc <= ch; cc++)
+      for (int bb = bl; bb <= bh; bb++) items[cursor[bb + nbB * cc]++] = (int)t;
+  }
+  const long strideA = A == 0 ? 1 : (A == 1 ? dim[0] : (long)dim[0] * dim[1]);
+  const long strideB = B == 0 ? 1 : (B == 1 ? dim[0] : (long)dim[0] * dim[1]);
+  const long strideC = C == 0 ? 1 : (C == 1 ? dim[0] : (long)dim[0] * dim[1]);
+  for (int ic = 0; ic < nC; ic++) {
+    const double pc = minC + (ic + 0.5003719) * cell;
+    const int bc = (int)fmin(nbC - 1, fmax(0, floor((pc - minC) * kC)));
+    for (int ib = 0; ib < nB; ib++) {
+      const double pb = minB + (ib + 0.4996281) * cell;
+      const int bb = (int)fmin(nbB - 1, fmax(0, floor((pb - minB) * kB)));
+      const int s = count[bb + nbB * bc], e = count[bb + nbB * bc + 1];
+      if (s == e) continue;
+      int nh = 0;
+      for (int k = s; k < e && nh < 512; k++) {
+        const float* o = P + 9 * (long)items[k];
+        const double b0 = o[B], c0 = o[C], b1 = o[3 + B], c1 = o[3 + C], b2 = o[6 + B], c2 = o[6 + C];
+        const double d = (c1 - c2) * (b0 - b2) + (b2 - b1) * (c0 - c2);
+        if (d == 0) continue;
+        const double id = 1 / d;
+        const double l0 = ((c1 - c2) * (pb - b2) + (b2 - b1) * (pc - c2)) * id;
+        if (l0 < 0 || l0 > 1) continue;
+        const double l1 = ((c2 - c0) * (pb - b2) + (b0 - b2) * (pc - c2)) * id;
+        if (l1 < 0 || l1 > 1) continue;
+        const double l2 = 1 - l0 - l1;
+        if (l2 < 0 || l2 > 1) continue;
+        hits[nh++] = l0 * (double)o[A] + l1 * (double)o[3 + A] + l2 * (double)o[6 + A];
+      }
+      if (nh < 2) continue;
+      qsort(hits, (size_t)nh, sizeof(double), or_cmp_double);
+      const long colBase = ib * strideB + ic * strideC;
+      for (int k = 0; k + 1 < nh; k += 2) {
+        double i0 = ceil((hits[k] - minA) / cell - 0.5);
+        double i1 = floor((hits[k + 1] - minA) / cell - 0.5);
+        if (i0 < 0) i0 = 0;
+        if (i1 >= nA) i1 = nA - 1;
+        for (double ia = i0; ia <= i1; ia++) votes[colBase + (long)ia * strideA]++;
+      }
+    }
+  }
+  free(count); free(lo); free(hi); free(hits); free(items); free(cursor);
+  return 0;
+}
+
+/* js/voxel.js:48-102: the grid (x fastest, nx*ny*nz bytes) and its stats. */
+int or_voxel_build(const float* P, long ntri, int res, uint8_t* grid, or_voxel_info* vi) {
+  int rc = or_voxel_dims(P, ntri, res, vi);
+  if (rc) return rc;
+  const long n = (long)vi->nx * vi->ny * vi->nz;
+  uint8_t* votes = (uint8_t*)calloc((size_t)n, 1);
+  uint8_t* shell = (uint8_t*)calloc((size_t)n, 1);
+  if (!votes || !shell) { free(votes); free(shell); return -4; }
+  or_raster_surface(P, ntri, shell, vi);
+  for (int axis = 0; axis < 3; axis++) {
+    if (or_parity_fill(P, ntri, votes, vi, axis)) { free(votes); free(shell); return -4; }
+  }
+  long solid = 0, disagree = 0;
+  for (long i = 0; i < n; i++) {
+    const int v = votes[i];
+    const int inside = v >= 2 || shell[i] == 1;
+    if (inside) solid++;
+    if (v == 1 || v == 2) disagree++;
+    grid[i] = inside ? 1 : 0;
+  }
+  vi->solid = solid;
+  vi->openness = solid ? (double)disagree / solid : 0;
+  free(votes); free(shell);
+  return 0;
+}
+
 #define OR_CAT2(a, b) a##b
 #define OR_CAT(a, b) OR_CAT2(a, b)
 

@@ -97,6 +97,10 @@ def lib() -> C.CDLL:
     L.or_lookup_mask.argtypes = [_U8, C.c_int, C.c_int, C.c_int, _D, C.c_double, _D, _D,
                                  C.c_double, C.c_int, C.c_int, C.c_int, _D, _U8]
     L.or_lookup_mask.restype = C.c_long
+    L.or_voxel_dims.argtypes = [_F, C.c_long, C.c_int, C.c_void_p]
+    L.or_voxel_dims.restype = C.c_int
+    L.or_voxel_build.argtypes = [_F, C.c_long, C.c_int, _U8, C.c_void_p]
+    L.or_voxel_build.restype = C.c_int
     L.or_uniform_draw.argtypes = [C.c_uint64, C.c_uint64]
     L.or_uniform_draw.restype = C.c_double
     L.or_toint32_export.argtypes = [C.c_double]
@@ -136,6 +140,33 @@ def lookup_mask(grid, gmin, ginv, M, P, scale, nx, ny, nz, box) -> np.ndarray:
                          _dp(np.ascontiguousarray(P, np.float64)), float(scale), nx, ny, nz,
                          _dp(_box6(box)), out.ctypes.data_as(_U8))
     return out
+
+
+class or_voxel_info(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("tris", C.c_int),
+                ("cell", C.c_double), ("inv", C.c_double), ("min", C.c_double * 3),
+                ("ext", C.c_double * 3), ("centre", C.c_double * 3), ("bbox", C.c_double * 6),
+                ("solid", C.c_long), ("openness", C.c_double)]
+
+
+def voxel_build(P, res: int = 96):
+    """Voxel.build (js/voxel.js:48-102): (grid [nz][ny][nx] uint8, info dict)."""
+    L = lib()
+    p = np.ascontiguousarray(P, np.float32).ravel()
+    ntri = p.size // 9
+    vi = or_voxel_info()
+    rc = L.or_voxel_dims(p.ctypes.data_as(_F), ntri, int(res), C.byref(vi))
+    if rc:
+        raise ValueError({-1: "Mesh has no triangles.", -2: "Mesh is degenerate (zero size).",
+                          -3: "Voxel grid too large; lower the resolution."}.get(rc, rc))
+    grid = np.zeros((vi.nz, vi.ny, vi.nx), np.uint8)
+    rc = L.or_voxel_build(p.ctypes.data_as(_F), ntri, int(res), grid.ctypes.data_as(_U8),
+                          C.byref(vi))
+    if rc:
+        raise ValueError(f"oracle voxel build failed ({rc})")
+    info = {k: (list(getattr(vi, k)) if k in ("min", "ext", "centre", "bbox") else
+                getattr(vi, k)) for k, _ in or_voxel_info._fields_}
+    return grid, info
 
 
 def uniform_draw(seed: int, k: int) -> float:

@@ -133,7 +133,7 @@ def test_exact_cfg0_shape_bit_identical(both, kernel):
     assert_bit_exact(g, o, np.float32)
 
 
-@pytest.mark.parametrize("kernel", ["direct", "staged", "vector", "pipe", "x2", "tma"])
+@pytest.mark.parametrize("kernel", ["direct", "staged", "vector", "pipe", "x2", "tma", "lean"])
 @pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
 def test_fast_f32_within_tolerance(both, side_bc, kernel):
     g, o = make_pair(both, (48, 24, 24), "f32", "fast", kernel=kernel,
@@ -182,7 +182,7 @@ def test_fast_cfg0_drag_and_fields(both):
     assert abs(clg - clo) <= 1e-3 * abs(cdo), (clg, clo)
 
 
-@pytest.mark.parametrize("kernel", ["direct", "staged", "vector", "pipe", "x2", "tma"])
+@pytest.mark.parametrize("kernel", ["direct", "staged", "vector", "pipe", "x2", "tma", "lean"])
 def test_f16dev_within_tolerance(both, kernel):
     g, o = make_pair(both, (48, 24, 24), "f16dev", "fast", kernel=kernel,
                      sphere=(14.0, 12.0, 12.0, 5.0))
@@ -197,7 +197,7 @@ def test_f16dev_within_tolerance(both, kernel):
 
 @pytest.mark.parametrize("math,kernel", [("fast", "direct"), ("fast", "vector"),
                                          ("fast", "pipe"), ("fast", "x2"), ("fast", "tma"),
-                                         ("exact", "direct")])
+                                         ("fast", "lean"), ("exact", "direct")])
 @pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
 def test_uniform_flow_is_preserved(both, math, kernel, side_bc):
     """A uniform stream past no body is a fixed point of the step (free-slip exactly)."""
@@ -236,7 +236,7 @@ def test_kernels_agree(both, storage, dims):
     differently only where the compiler contracts a multiply-add differently."""
     LBM, _ = both
     nx = dims[0]
-    kernels = ["direct", "vector", "pipe", "x2"]
+    kernels = ["direct", "vector", "pipe", "x2"]   # the lean kernel needs stationary walls
     kernels += ["staged"] if nx % STAGE_VEC[storage] == 0 else []
     kernels += ["tma"] if nx % TMA_VEC[storage] == 0 else []
     sims = []
@@ -255,21 +255,24 @@ def test_kernels_agree(both, storage, dims):
         assert np.abs(pa - pb).max() <= (1e-6 if storage == "f32" else 1e-4)
 
 
-@pytest.mark.parametrize("kernel", ["x2", "tma"])
+@pytest.mark.parametrize("kernel,moving", [("x2", True), ("tma", True), ("x2", False),
+                                           ("tma", False), ("lean", False)])
 @pytest.mark.parametrize("storage", ["f32", "f16dev"])
 @pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
-def test_packed_kernels_agree_with_direct_moving_walls(both, kernel, storage, side_bc):
-    """The packed two-cell kernels against the direct kernel with every special
+def test_packed_kernels_agree_with_direct_moving_walls(both, kernel, moving, storage, side_bc):
+    """The packed and lean kernels against the direct kernel with every special
     rule active: a spinning body (moving-wall correction reading the previous
-    step's density), a rolling road, the body touching the outlet column and
-    the side planes; fields are checked on an intermediate and the last step."""
+    step's density) and a rolling road, or stationary ones, the body touching
+    the outlet column, and the side planes; fields are checked on an
+    intermediate and the last step."""
     LBM, _ = both
     dims = (40, 14, 12)
     out = []
     for kern in ("direct", kernel):
         s = LBM(*dims, storage=storage, kernel=kern, side_bc=side_bc)
-        apply_case(s, sphere=(36.5, 6.0, 6.0, 3.4), side_bc=side_bc, ground=True, roadVel=0.03,
-                   wallVel=spinning_sphere_wallvel(36.5, 6.0, 6.0, 0.01))
+        apply_case(s, sphere=(36.5, 6.0, 6.0, 3.4), side_bc=side_bc, ground=True,
+                   roadVel=0.03 if moving else 0.0,
+                   wallVel=spinning_sphere_wallvel(36.5, 6.0, 6.0, 0.01) if moving else None)
         f1 = s.step_forces(7)
         u1 = s.fields()
         f2 = s.step_forces(20)

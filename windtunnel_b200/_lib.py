@@ -40,6 +40,7 @@ WT_KERNEL_VECTOR = 3
 WT_KERNEL_PIPE = 4
 WT_KERNEL_X2 = 5
 WT_KERNEL_TMA = 6
+WT_KERNEL_LEAN = 7
 
 WT_ROUND_NEAREST = 0
 WT_ROUND_STOCHASTIC = 1
@@ -100,6 +101,13 @@ class wt_adj_stats(C.Structure):
                 ("device_bytes", C.c_int64), ("checkpoints", C.c_int32), ("segment", C.c_int32)]
 
 
+class wt_voxel_info(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("reserved", C.c_int32),
+                ("tris", C.c_int64), ("cell", C.c_double), ("inv", C.c_double),
+                ("min", C.c_double * 3), ("ext", C.c_double * 3), ("centre", C.c_double * 3),
+                ("bbox", C.c_double * 6), ("solid", C.c_int64), ("openness", C.c_double)]
+
+
 class WTError(RuntimeError):
     """A wt_* call returned a negative status."""
 
@@ -148,8 +156,13 @@ SIGNATURES = {
     "wt_get_launch_count": [_P, C.POINTER(C.c_int64)],
     "wt_set_solid_fraction": [_P, _I, _D],
     "wt_adjoint": [_P, C.POINTER(wt_adj_cfg), _D, C.POINTER(wt_adj_stats)],
+    "wt_voxel_dims": [C.POINTER(C.c_float), C.c_int64, C.c_int, C.POINTER(wt_voxel_info)],
+    "wt_voxel_build": [C.POINTER(C.c_float), C.c_int64, C.c_int, C.POINTER(C.c_uint8), C.c_size_t,
+                       C.POINTER(wt_voxel_info)],
+    "wt_voxel_last_error": [],
 }
-_RESTYPES = {"wt_default_params": None, "wt_last_error": C.c_char_p}
+_RESTYPES = {"wt_default_params": None, "wt_last_error": C.c_char_p,
+             "wt_voxel_last_error": C.c_char_p}
 
 _lib: C.CDLL | None = None
 

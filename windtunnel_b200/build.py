@@ -33,6 +33,7 @@ UNITS = {
     "wt_kernels_fast.cu": [],
     "wt_kernels_exact.cu": ["--fmad=false"],
     "wt_api.cu": [],
+    "wt_voxel.cu": ["--fmad=false"],
 }
 
 

@@ -86,7 +86,7 @@ int check_params(const wt_params* p) {
   if (p->trt && !(p->lambda > 0)) return WT_ERR_ARG;
   if (p->side_bc != WT_SIDE_EQ && p->side_bc != WT_SIDE_FREESLIP) return WT_ERR_ARG;
   if (p->math != WT_MATH_FAST && p->math != WT_MATH_EXACT) return WT_ERR_ARG;
-  if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_TMA) return WT_ERR_ARG;
+  if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_LEAN) return WT_ERR_ARG;
   if (p->f16_rounding != WT_ROUND_NEAREST && p->f16_rounding != WT_ROUND_STOCHASTIC)
     return WT_ERR_ARG;
   if (p->reserved != 0) return WT_ERR_ARG;
@@ -131,10 +131,13 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
   a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
   a.n = h->n;
   a.nxy = (long long)h->nx * h->ny;
+  const bool narrow = 19 * h->n * (long long)sizeof(S) < (1LL << 31);
   for (int q = 0; q < 19; q++) {
     const long long off = wt::ex(q) + (long long)h->nx * wt::ey(q) + a.nxy * wt::ez(q);
     a.src[q] = q * h->n - off;
     a.dst[q] = q * h->n;
+    a.srcb[q] = narrow ? (int)(a.src[q] * (long long)sizeof(S)) : 0;
+    a.dstb[q] = narrow ? (int)(a.dst[q] * (long long)sizeof(S)) : 0;
   }
   const wt_params& p = h->p;
   a.tau0 = p.tau;
@@ -164,11 +167,12 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
 // direction block starts on a 16-byte boundary.
 bool staged_ok(const wt_lattice* h) { return h->nx % (int)(16 / h->elem) == 0; }
 
-enum class Path { Direct, Staged, Vector, Pipe, X2, Tma, Pbb };
+enum class Path { Direct, Staged, Vector, Pipe, X2, Tma, Pbb, Lean };
 
-template <class S, class L, class LS, class LV, class LP, class LX, class LT, class LB>
+template <class S, class L, class LS, class LV, class LP, class LX, class LT, class LB, class LL>
 void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged, LV launch_vec,
-               LP launch_pipe, LX launch_x2, LT launch_tma, LB launch_pbb, double* forces_dev) {
+               LP launch_pipe, LX launch_x2, LT launch_tma, LB launch_pbb, LL launch_lean,
+               double* forces_dev) {
   wt::StepArgs<S> a = make_args<S>(h);
   const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
   const bool wide = 19 * h->n >= (1LL << 31);
@@ -188,6 +192,7 @@ void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged,
         case Path::X2: launch_x2(a, wide, h->stream); break;
         case Path::Tma: launch_tma(a, *h->tma, h->parity, h->stream); break;
         case Path::Pbb: launch_pbb(a, grid, wide, h->stream); break;
+        case Path::Lean: launch_lean(a, grid, wide, h->stream); break;
         default: launch(a, grid, wide, h->stream); break;
       }
       h->launches++;
@@ -207,10 +212,25 @@ bool x2_ok(const wt_lattice* h) {
   return !exact && !sr && h->nx % 2 == 0;
 }
 
-// The kernel WT_KERNEL_AUTO runs: the direct kernel for now.
+bool lean_ok(const wt_lattice* h);
+
+// The kernel WT_KERNEL_AUTO runs, the fastest measured on B200 for the form
+// (256x128x128 channel): half storage, the lean kernel (37-42k MLUPS against
+// 33k for the direct one); float32 storage and the exact collision, the
+// direct kernel (33.5k against 31.8k for lean).
 Path auto_path(const wt_lattice* h) {
-  (void)h;
+  if (h->storage == WT_STORE_F16DEV && lean_ok(h)) return Path::Lean;
   return Path::Direct;
+}
+
+// True when the lean-addressing kernel can run.
+// Moving walls are excluded: their correction reads the previous step's
+// density, which the thread of cell nx-2 rewrites while the outlet thread
+// recomputes that cell.
+bool lean_ok(const wt_lattice* h) {
+  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
+  const bool sr = h->storage == WT_STORE_F16DEV && h->p.f16_rounding == WT_ROUND_STOCHASTIC;
+  return !exact && !sr && !h->p.moving_walls && 19 * h->n * (long long)h->elem < (1LL << 31);
 }
 
 // True when the TMA tile kernel can run.
@@ -645,6 +665,13 @@ int select_path(wt_lattice* h, Path* out) {
                     "element (4 float32, 8 half) and nearest rounding for half storage");
       path = Path::Tma;
       break;
+    case WT_KERNEL_LEAN:
+      if (!lean_ok(h))
+        return fail(h, WT_ERR_UNSUPPORTED,
+                    "the lean kernel needs the float32 collision, buffers under 2 GiB, "
+                    "stationary walls and nearest rounding for half storage");
+      path = Path::Lean;
+      break;
     case WT_KERNEL_AUTO:
       path = auto_path(h);
       break;
@@ -663,20 +690,22 @@ void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* forces_dev) {
       if (exact) run_steps<float>(h, nsteps, path, wt::launch_step_f32_exact,
                                   wt::launch_staged_f32_exact, no_vec<float>, no_vec<float>,
                                   no_vec<float>, no_tma<float>, wt::launch_pbb_f32_exact,
-                                  forces_dev);
+                                  wt::launch_step_f32_exact, forces_dev);
       else run_steps<float>(h, nsteps, path, wt::launch_step_f32_fast, wt::launch_staged_f32_fast,
                             wt::launch_vec_f32, wt::launch_pipe_f32, wt::launch_x2_f32,
-                            wt::launch_tma_f32, wt::launch_pbb_f32_fast, forces_dev);
+                            wt::launch_tma_f32, wt::launch_pbb_f32_fast, wt::launch_lean_f32,
+                            forces_dev);
       break;
     case WT_STORE_F16DEV:
       run_steps<__half>(h, nsteps, path, wt::launch_step_f16_fast, wt::launch_staged_f16_fast,
                         wt::launch_vec_f16, wt::launch_pipe_f16, wt::launch_x2_f16,
-                        wt::launch_tma_f16, wt::launch_pbb_f16_fast, forces_dev);
+                        wt::launch_tma_f16, wt::launch_pbb_f16_fast, wt::launch_lean_f16,
+                        forces_dev);
       break;
     default:
       run_steps<double>(h, nsteps, path, wt::launch_step_f64_exact, wt::launch_staged_f64_exact,
                         no_vec<double>, no_vec<double>, no_vec<double>, no_tma<double>,
-                        wt::launch_pbb_f64_exact, forces_dev);
+                        wt::launch_pbb_f64_exact, wt::launch_step_f64_exact, forces_dev);
       break;
   }
 }
@@ -1191,8 +1220,10 @@ extern "C" int wt_step_noalloc(wt_lattice* h, int nsteps, double* forces) {
                 "wt_step_noalloc: the body has " + std::to_string(h->nslots) +
                     " wall segments, more than the " + std::to_string(kNaSlots) +
                     " its fixed scratch holds; use wt_step");
-  if (h->p.kernel != WT_KERNEL_AUTO && h->p.kernel != WT_KERNEL_DIRECT)
-    return fail(h, WT_ERR_UNSUPPORTED, "wt_step_noalloc runs the direct kernel only");
+  if (h->p.kernel != WT_KERNEL_AUTO && h->p.kernel != WT_KERNEL_DIRECT &&
+      h->p.kernel != WT_KERNEL_LEAN)
+    return fail(h, WT_ERR_UNSUPPORTED,
+                "wt_step_noalloc runs the direct or lean kernel only (the one-cell kernels)");
   if (h->sfrac)
     return fail(h, WT_ERR_UNSUPPORTED, "wt_step_noalloc does not run partial bounce-back");
   int dev = -1;
@@ -1211,13 +1242,19 @@ extern "C" int wt_step_noalloc(wt_lattice* h, int nsteps, double* forces) {
   // partial slot and every force entry is written before it is read.
   WT_CUDA(h, cudaMemsetAsync(err, 0, 8 + 4 * sizeof(long long), h->stream));
   const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
+  Path path = Path::Direct;
+  c = select_path(h, &path);   // the kernel wt_step runs for these parameters
+  if (c != WT_OK) return c;
+  const bool lean = path == Path::Lean;
   switch (h->storage) {
     case WT_STORE_F32:
       if (exact) run_steps_noalloc<float>(h, nsteps, wt::launch_step_f32_exact, part, fdev, err, diag);
+      else if (lean) run_steps_noalloc<float>(h, nsteps, wt::launch_lean_f32, part, fdev, err, diag);
       else run_steps_noalloc<float>(h, nsteps, wt::launch_step_f32_fast, part, fdev, err, diag);
       break;
     case WT_STORE_F16DEV:
-      run_steps_noalloc<__half>(h, nsteps, wt::launch_step_f16_fast, part, fdev, err, diag);
+      if (lean) run_steps_noalloc<__half>(h, nsteps, wt::launch_lean_f16, part, fdev, err, diag);
+      else run_steps_noalloc<__half>(h, nsteps, wt::launch_step_f16_fast, part, fdev, err, diag);
       break;
     default:
       run_steps_noalloc<double>(h, nsteps, wt::launch_step_f64_exact, part, fdev, err, diag);

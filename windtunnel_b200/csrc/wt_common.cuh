@@ -121,6 +121,8 @@ struct StepArgs {
   long long nxy;       // nx*ny
   long long src[Q];    // pull offset of direction q: q*n - (ex + nx*ey + nxy*ez)
   long long dst[Q];    // store offset of direction q: q*n
+  int srcb[Q];         // src[q] and dst[q] in bytes, when both buffers span < 2^31 bytes
+  int dstb[Q];
   // float64 parameters (exact collision)
   double tau0, omega0, cs2, lam;
   // float32 parameters (fast collision), rounded once on the host

@@ -8,6 +8,7 @@
 #include "wt_x2.cuh"
 #include "wt_tma.cuh"
 #include "wt_pbb.cuh"
+#include "wt_lean.cuh"
 
 #include <algorithm>
 
@@ -45,6 +46,14 @@ void launch_x2_f16(const StepArgs<__half>& a, bool wide, cudaStream_t s) {
   const dim3 g = x2_grid(a.nx, a.ny, a.nz);
   if (wide) k_step_x2<__half, long long><<<g, X2_BX, 0, s>>>(a);
   else k_step_x2<__half, int><<<g, X2_BX, 0, s>>>(a);
+}
+
+void launch_lean_f32(const StepArgs<float>& a, dim3 grid, bool, cudaStream_t s) {
+  k_step_lean<float><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool, cudaStream_t s) {
+  k_step_lean<__half><<<grid, STEP_BX, 0, s>>>(a);
 }
 
 // ---- partial bounce-back and adjoint (float32 arithmetic) -------------------------

@@ -1,0 +1,89 @@
+// wt_lean.cuh — the fused step, one thread per cell, with lean addressing.
+//
+// Same semantics and per-cell rules as k_step (wt_step.cuh); the arithmetic
+// is collide_x2 on one cell (scaled storage units, approximate reciprocal and
+// square root, wt_x2.cuh). What differs is how the 38 population accesses of
+// a cell are addressed: every thread forms one byte pointer to its cell in
+// the read buffer and one in the write buffer, and each access adds a 32-bit
+// byte offset that is the same for every thread of the launch (StepArgs
+// srcb / dstb). A direction therefore costs one load or store plus at most
+// one add, instead of a 64-bit multiply-add chain per access. Used when both
+// population buffers span less than 2^31 bytes. The outlet column is computed
+// by its own threads (a recomputation of column nx-2), so the common path has
+// no second store per population.
+#pragma once
+
+#include "wt_x2.cuh"
+
+namespace wt {
+
+template <class S>
+__global__ void __launch_bounds__(STEP_BX, 8) k_step_lean(const __grid_constant__ StepArgs<S> a) {
+  using T = X2<S>;
+  constexpr float SC = T::SC;
+  const int x = blockIdx.x * STEP_BX + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z;
+  double Fx = 0, Fy = 0, Fz = 0;
+  bool near_cell = false;
+  if (x < a.nx) {
+    // The outlet column x = nx-1 holds a copy of column nx-2 after the step
+    // (js/lbm.js:504-511): its thread recomputes cell nx-2 and writes its own
+    // cell, so no thread stores twice.
+    const bool outlet = x == a.nx - 1;
+    const int xs = outlet ? a.nx - 2 : x;
+    const long long row = (long long)a.nx * y + a.nxy * z;
+    const long long is = xs + row, id = x + row;
+    int cat;
+    uint8_t fl = 0;
+    if (xs == 0) {
+      cat = CAT_EQ;
+    } else {
+      fl = a.flags[is];
+      if (z == 0 || z == a.nz - 1 || y == a.ny - 1) cat = CAT_EQ;
+      else if (fl & FLAG_SOLID_MASK) cat = CAT_KEEP;
+      else if (y == 0) cat = CAT_EQ;
+      else cat = CAT_FLUID;
+    }
+    char* Gb = reinterpret_cast<char*>(a.G + id);
+    auto gs = [&](int q) -> S& { return *reinterpret_cast<S*>(Gb + a.dstb[q]); };
+    if (cat == CAT_FLUID) {
+      const char* Fb = reinterpret_cast<const char*>(a.F + is);
+      float f[Q];
+#pragma unroll
+      for (int q = 0; q < Q; q++) f[q] = T::raw(*reinterpret_cast<const S*>(Fb + a.srcb[q]));
+      const bool wall = (fl & FLAG_NEAR) != 0;
+      const bool shell = a.freeslip && (y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2);
+      if (wall || shell) patch_raw<S, 0>(a, is, xs, y, z, wall, shell, f, Fx, Fy, Fz);
+      near_cell = wall && !outlet;   // the copy's links are not counted twice
+      float r, vx, vy, vz;
+      collide_x2<S, float>(a, f, r, vx, vy, vz);
+      if (!(r > 0.0f && r < 3.0e38f)) atomicOr(a.err, 1u);
+      if (a.write_fields) {
+        a.rho[id] = r * (1.0f / SC); a.ux[id] = vx; a.uy[id] = vy; a.uz[id] = vz;
+      } else if (a.mov && near_cell) {
+        a.rho[is] = r * (1.0f / SC);
+      }
+#pragma unroll
+      for (int q = 0; q < Q; q++) gs(q) = T::to_s(f[q]);
+    } else if (cat == CAT_EQ) {
+#pragma unroll
+      for (int q = 0; q < Q; q++) gs(q) = a.eq[q];
+      if (a.write_fields) {
+        a.ux[id] = a.u0f; a.uy[id] = 0.0f; a.uz[id] = 0.0f; a.rho[id] = 1.0f;
+      }
+    } else if (outlet) {
+      // copy of a solid cell in column nx-2: its g is not written this step
+      const char* Gs = reinterpret_cast<const char*>(a.G + is);
+#pragma unroll
+      for (int q = 0; q < Q; q++) gs(q) = *reinterpret_cast<const S*>(Gs + a.dstb[q]);
+      if (a.write_fields) {
+        a.ux[id] = a.ux[is]; a.uy[id] = a.uy[is]; a.uz[id] = a.uz[is]; a.rho[id] = a.rho[is];
+      }
+    }
+    if (!near_cell) Fx = Fy = Fz = 0.0;
+  }
+  constexpr double inv_sc = 1.0 / (double)SC;   // a power of two: exact
+  warp_force_partial(Fx * inv_sc, Fy * inv_sc, Fz * inv_sc, near_cell, a);
+}
+
+}  // namespace wt

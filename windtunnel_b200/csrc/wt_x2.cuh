@@ -66,10 +66,29 @@ __device__ __forceinline__ float sqrt_approx(float x) {
 __device__ __forceinline__ f2 prcp(f2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
 __device__ __forceinline__ f2 psqrt(f2 a) { return make_float2(sqrt_approx(a.x), sqrt_approx(a.y)); }
 
+// The same operations on one cell (a scalar float), so that the collision
+// below also serves the one-cell-per-thread kernels.
+template <class V>
+__device__ __forceinline__ V splat(float a);
+template <>
+__device__ __forceinline__ f2 splat<f2>(float a) { return pk(a); }
+template <>
+__device__ __forceinline__ float splat<float>(float a) { return a; }
+__device__ __forceinline__ float padd(float a, float b) { return a + b; }
+__device__ __forceinline__ float psub(float a, float b) { return a - b; }
+__device__ __forceinline__ float pmul(float a, float b) { return a * b; }
+__device__ __forceinline__ float pfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ float prcp(float a) { return rcp_approx(a); }
+__device__ __forceinline__ float psqrt(float a) { return sqrt_approx(a); }
+
 template <int C>
 __device__ __forceinline__ float& lane_of(f2& v) {
   if constexpr (C == 0) return v.x;
   else return v.y;
+}
+template <int C>
+__device__ __forceinline__ float& lane_of(float& v) {
+  return v;
 }
 
 // Storage in scaled units: raw(v) is the stored number as a float (the
@@ -99,9 +118,9 @@ struct X2<__half> {
 // (js/lbm.js:334-368 for the bounce-back links; k_step's patch_special is
 // the same rule in deviation units). The momentum exchange accumulates in
 // raw units; the caller divides by SC.
-template <class S, int C>
+template <class S, int C, class VV>
 __device__ __forceinline__ void patch_raw(const StepArgs<S>& a, long long i, int x, int y, int z,
-                                          bool near_cell, bool shell, f2 (&f)[Q], double& Fx,
+                                          bool near_cell, bool shell, VV (&f)[Q], double& Fx,
                                           double& Fy, double& Fz) {
   using T = X2<S>;
   const unsigned long long m = near_cell ? a.nmask[i] : 0ull;
@@ -143,10 +162,11 @@ __device__ __forceinline__ void patch_raw(const StepArgs<S>& a, long long i, int
 // Packed collision of two cells in raw (scaled) units: f -> g, with the
 // density r~ = SC * rho and the velocity of each lane. The mathematics is
 // that of js/lbm.js:377-460 (collide_fast's re-association).
-template <class S>
+template <class S, class f2 = wt::f2>
 __device__ __forceinline__ void collide_x2(const StepArgs<S>& a, f2 (&f)[Q], f2& r, f2& vx,
                                            f2& vy, f2& vz) {
   constexpr float SC = X2<S>::SC;
+  auto pk = [](float v) { return splat<f2>(v); };
   const f2 s1 = padd(f[1], f[2]), d1 = psub(f[1], f[2]);
   const f2 s3 = padd(f[3], f[4]), d3 = psub(f[3], f[4]);
   const f2 s5 = padd(f[5], f[6]), d5 = psub(f[5], f[6]);
