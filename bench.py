@@ -451,12 +451,13 @@ def adjoint_study(aw) -> dict:
         "J_rel": abs(J - Jr) / abs(Jr)}
     if aw["fd_cells"]:
         rng = np.random.default_rng(aw["seed"] + 1)
-        shape = g.shape
         s0 = design_field(aw)
         eps = aw["fd_eps"]
+        # seeded cells whose +-eps perturbation stays inside [0, 1]
+        free = np.argwhere((s0 > eps) & (s0 < 1 - eps))
+        pick = free[rng.choice(len(free), aw["fd_cells"], replace=False)]
         rows = []
-        for _ in range(aw["fd_cells"]):
-            idx = tuple(int(rng.integers(0, n)) for n in shape)
+        for idx in map(tuple, pick):
             js = []
             for sgn in (1, -1):
                 sv = s0.copy()

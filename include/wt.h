@@ -330,6 +330,22 @@ int wt_sample(wt_lattice* h, const double* xyz, int npts, double* out);
 /* LBM.isSolid(x, y, z) — js/lbm.js:541-545. */
 int wt_is_solid(wt_lattice* h, double x, double y, double z, int* out);
 
+/* The scalar the reference's slice view colours (js/main.js:925-968), for
+ * every cell of one lattice plane: plane 0 is the xy plane z = k, plane 1
+ * the xz plane y = k; field 0 = |u| / u0, 1 = pressure coefficient of the
+ * 5-point averaged density ((rho - 1) / 3) / (u0^2 / 2), 2 = in-plane
+ * vorticity / u0 (central differences). out holds nx * (ny or nz) floats,
+ * x fastest; solid cells are NaN. The colour map itself is the caller's. */
+int wt_slice(wt_lattice* h, int plane, int k, int field, float* out, size_t len);
+
+/* One step of the reference's smoke particles (js/main.js:691-709) for n
+ * particles: xyz (3n doubles, lattice coordinates) moves by the trilinear
+ * velocity of LBM.sample times kstep; expired[p] (optional) = 1 when the
+ * particle left the margins of js/main.js:701-702 or entered a solid cell;
+ * speed[p] (optional) = |u| / u0 at its old position. Ages, respawning and
+ * colours stay with the caller. */
+int wt_advect(wt_lattice* h, double* xyz, int n, double kstep, uint8_t* expired, float* speed);
+
 /* The handle's CUDA stream (a cudaStream_t), for timing with events. */
 int wt_get_stream(const wt_lattice* h, void** stream);
 

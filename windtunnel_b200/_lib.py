@@ -160,6 +160,8 @@ SIGNATURES = {
     "wt_voxel_build": [C.POINTER(C.c_float), C.c_int64, C.c_int, C.POINTER(C.c_uint8), C.c_size_t,
                        C.POINTER(wt_voxel_info)],
     "wt_voxel_last_error": [],
+    "wt_slice": [_P, C.c_int, C.c_int, C.c_int, _F, C.c_size_t],
+    "wt_advect": [_P, _D, C.c_int, C.c_double, _U8, _F],
 }
 _RESTYPES = {"wt_default_params": None, "wt_last_error": C.c_char_p,
              "wt_voxel_last_error": C.c_char_p}

@@ -34,6 +34,7 @@ UNITS = {
     "wt_kernels_exact.cu": ["--fmad=false"],
     "wt_api.cu": [],
     "wt_voxel.cu": ["--fmad=false"],
+    "wt_view.cu": ["--fmad=false"],
 }
 
 

@@ -385,6 +385,31 @@ class LBM:
     def g(self) -> np.ndarray:
         return self.populations("g")
 
+    # ---- visualisation arithmetic (js/main.js:691-709, :925-968) ---------------------------
+    def slice(self, plane: str = "xy", k: int | None = None, field: str = "speed") -> np.ndarray:
+        """The slice view's scalar on plane 'xy' (z = k) or 'xz' (y = k): field 'speed'
+        (|u|/u0), 'pressure' (Cp) or 'vorticity' (/u0); NaN on solid cells."""
+        p = {"xy": 0, "xz": 1}[plane]
+        if k is None:
+            k = (self.nz if p == 0 else self.ny) // 2
+        h = self.ny if p == 0 else self.nz
+        out = np.empty((h, self.nx), np.float32)
+        f = {"speed": 0, "pressure": 1, "vorticity": 2}[field]
+        self._call(lib().wt_slice, p, int(k), f, out.ctypes.data_as(C.POINTER(C.c_float)),
+                   out.size)
+        return out
+
+    def advect(self, xyz: np.ndarray, kstep: float):
+        """One smoke-particle step: (new positions (n, 3), expired (n,) bool, speed (n,))."""
+        p = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3).copy()
+        n = p.shape[0]
+        expired = np.zeros(n, np.uint8)
+        speed = np.zeros(n, np.float32)
+        self._call(lib().wt_advect, _dptr(p), n, float(kstep),
+                   expired.ctypes.data_as(C.POINTER(C.c_uint8)),
+                   speed.ctypes.data_as(C.POINTER(C.c_float)))
+        return p, expired.astype(bool), speed
+
     # ---- partial bounce-back and its adjoint (no reference counterpart) ------------------
     def set_solid_fraction(self, box, s) -> None:
         """Solid fraction on the half-open box (x0, y0, z0, x1, y1, z1); s is indexed
