@@ -72,8 +72,8 @@ enum {
 
 /* Which step kernel runs. */
 enum {
-  WT_KERNEL_AUTO = 0,    /* the kernel measured fastest on B200 for the form: LEAN for half
-                            storage (when it can run), DIRECT otherwise */
+  WT_KERNEL_AUTO = 0,    /* the kernel measured fastest on B200 for the form: LEAN when it
+                            can run, DIRECT otherwise */
   WT_KERNEL_DIRECT = 1,  /* one thread per cell, populations gathered straight from HBM */
   WT_KERNEL_STAGED = 2,  /* persistent CTAs staging the 19 pull rows with bulk copies (TMA);
                             needs nx to be a multiple of 16 bytes / element size */
@@ -90,8 +90,10 @@ enum {
                             nearest rounding for half storage */
   WT_KERNEL_LEAN = 7     /* one thread per cell, 32-bit byte offsets from one pointer per cell,
                             the collision in storage units with approximate reciprocal / square
-                            root; float32 collision, buffers under 2 GiB, stationary walls,
-                            nearest rounding for half storage */
+                            root, and an L2 prefetch of the populations a fixed distance
+                            ahead in launch order (environment WT_PREFETCH_CELLS overrides
+                            the distance at wt_create; 0 turns it off); float32 collision,
+                            buffers under 2 GiB, stationary walls */
 };
 
 /* Rounding of half-precision stores. Stochastic rounding draws its random
@@ -239,7 +241,9 @@ typedef struct wt_adj_cfg {
   int32_t nsteps;      /* forward steps from the current state */
   int32_t window;      /* J = mean of the force component over the last `window` steps */
   int32_t component;   /* 0 = x (drag), 1 = y, 2 = z */
-  int32_t checkpoint;  /* steps between stored states; 0 = ceil(sqrt(nsteps)) */
+  int32_t checkpoint;  /* steps between stored states; 0 = every state when
+                          (nsteps + 3) states fit in 3/4 of the free device
+                          memory, else ceil(sqrt(nsteps)) */
   int32_t reserved[4]; /* must be 0 */
 } wt_adj_cfg;
 
@@ -248,7 +252,7 @@ typedef struct wt_adj_stats {
   double forward_ms;   /* forward sweep with checkpoint copies (CUDA events) */
   double backward_ms;  /* recomputation + adjoint steps (CUDA events) */
   int64_t device_bytes;/* device memory the run allocated (checkpoints, segment, adjoint) */
-  int32_t checkpoints; /* stored states */
+  int32_t checkpoints; /* checkpoint intervals */
   int32_t segment;     /* steps per checkpoint interval */
 } wt_adj_stats;
 
@@ -256,7 +260,8 @@ typedef struct wt_adj_stats {
  * Runs cfg->nsteps steps from the current state (the lattice ends where
  * wt_step(h, nsteps) would leave it) storing a checkpoint every
  * cfg->checkpoint steps, then runs the adjoint backwards, recomputing each
- * interval's states from its checkpoint. dJds receives one double per cell
+ * interval's states from its checkpoint; the last interval's states are kept
+ * from the forward sweep, so with checkpoint == nsteps nothing is recomputed. dJds receives one double per cell
  * of the solid-fraction box (x fastest). Adjoint arithmetic: float64 for
  * float64 storage or WT_MATH_EXACT, float32 otherwise. Stationary walls only
  * (WT_ERR_UNSUPPORTED with moving walls); WT_ERR_STATE without a field. */

@@ -78,6 +78,20 @@ def test_adjoint_f64_reproduces_oracle(wt_lib, oracle_lib):
         assert np.array_equal(gc, gg), c
 
 
+@pytest.mark.parametrize("checkpoint", [6, 40])
+def test_adjoint_leaves_the_stepped_state(wt_lib, checkpoint):
+    """The lattice ends where step(nsteps) leaves it, whether the last
+    interval's states went through the segment store or not."""
+    N, W = 40, 15
+    g, r = _gpu("f32"), _gpu("f32")
+    J, _, _ = g.adjoint(N, W, checkpoint=checkpoint)
+    F = r.step_forces(N)
+    assert J == pytest.approx(F[-W:, 0].mean(), rel=1e-12)
+    assert np.array_equal(g.populations("f", "raw"), r.populations("f", "raw"))
+    for x, y in zip(g.fields(), r.fields()):
+        assert np.array_equal(x, y)
+
+
 def test_adjoint_f32_close_to_f64(wt_lib, oracle_lib):
     N, W = 40, 15
     _, gf, _ = _gpu("f32", math="fast").adjoint(N, W)

@@ -284,6 +284,51 @@ def test_packed_kernels_agree_with_direct_moving_walls(both, kernel, moving, sto
     assert np.abs(pa - pb).max() <= (1e-6 if storage == "f32" else 1e-4)
 
 
+def test_lean_stochastic_rounding_agrees_with_direct(both):
+    """Half storage with stochastic rounding: the lean kernel draws the direct
+    kernel's random bits for the same cell and step, so the two agree to the
+    half-storage tolerance of the other kernel comparisons, and the outlet
+    column stays an exact copy of column nx-2."""
+    LBM, _ = both
+    dims = (40, 14, 12)
+    out = []
+    for kern in ("direct", "lean"):
+        s = LBM(*dims, storage="f16dev", kernel=kern, side_bc="freeslip")
+        s.set_params(f16_rounding="stochastic")
+        apply_case(s, sphere=(20.0, 6.0, 6.0, 3.4), side_bc="freeslip", ground=True)
+        f = s.step_forces(25)
+        p = s.populations("f", "raw").reshape(19, dims[2], dims[1], dims[0])
+        assert np.array_equal(p[:, 1:-1, 1:-1, -1], p[:, 1:-1, 1:-1, -2])
+        out.append((f, s.fields(), s.populations("f", "f32")))
+    (fa, ua, pa), (fb, ub, pb) = out
+    assert np.abs(fa - fb).max() <= 1e-3 * np.abs(fa).max()
+    for a, b in zip(ua, ub):
+        assert np.abs(a - b).max() <= 2e-4
+    assert np.abs(pa - pb).max() <= 1e-4
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16dev"])
+def test_lean_prefetch_changes_nothing(both, storage, monkeypatch):
+    """The lean kernel's L2 prefetch distance (read at create time) moves
+    timing only: off, the default and one past the end of the lattice give
+    bit-identical populations and forces."""
+    LBM, _ = both
+    dims = (64, 20, 18)
+    out = []
+    for pf in ("0", None, str(64 * 20 * 18 * 2)):
+        if pf is None:
+            monkeypatch.delenv("WT_PREFETCH_CELLS", raising=False)
+        else:
+            monkeypatch.setenv("WT_PREFETCH_CELLS", pf)
+        s = LBM(*dims, storage=storage, kernel="lean", side_bc="freeslip")
+        apply_case(s, sphere=(40.0, 10.0, 9.0, 4.2), side_bc="freeslip", ground=True)
+        out.append((s.step_forces(25), s.populations("f", "raw")))
+    monkeypatch.delenv("WT_PREFETCH_CELLS", raising=False)
+    for f, p in out[1:]:
+        assert np.array_equal(f, out[0][0])
+        assert np.array_equal(p, out[0][1])
+
+
 def test_step_is_deterministic(both):
     LBM, _ = both
     runs = []

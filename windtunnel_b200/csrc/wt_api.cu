@@ -160,6 +160,7 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
   for (int q = 0; q < 19; q++) a.eq[q] = to_store<S>(eq[q]);
   a.sfrac = h->sfrac;
   for (int k = 0; k < 6; k++) a.sb[k] = h->sbox[k];
+  a.pf = h->pf;   // read by the lean kernel only
   return a;
 }
 
@@ -215,11 +216,12 @@ bool x2_ok(const wt_lattice* h) {
 bool lean_ok(const wt_lattice* h);
 
 // The kernel WT_KERNEL_AUTO runs, the fastest measured on B200 for the form
-// (256x128x128 channel): half storage, the lean kernel (37-42k MLUPS against
-// 33k for the direct one); float32 storage and the exact collision, the
-// direct kernel (33.5k against 31.8k for lean).
+// (256x128x128 channel): the lean kernel with its L2 prefetch where it can
+// run (float32 35.1k MLUPS against 33.4k for the direct kernel, half 42.3k
+// against 37.1k), the direct kernel otherwise (exact collision, float64,
+// moving walls, buffers of 2^31 bytes or more).
 Path auto_path(const wt_lattice* h) {
-  if (h->storage == WT_STORE_F16DEV && lean_ok(h)) return Path::Lean;
+  if (lean_ok(h)) return Path::Lean;
   return Path::Direct;
 }
 
@@ -229,8 +231,7 @@ Path auto_path(const wt_lattice* h) {
 // recomputes that cell.
 bool lean_ok(const wt_lattice* h) {
   const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
-  const bool sr = h->storage == WT_STORE_F16DEV && h->p.f16_rounding == WT_ROUND_STOCHASTIC;
-  return !exact && !sr && !h->p.moving_walls && 19 * h->n * (long long)h->elem < (1LL << 31);
+  return !exact && !h->p.moving_walls && 19 * h->n * (long long)h->elem < (1LL << 31);
 }
 
 // True when the TMA tile kernel can run.
@@ -348,6 +349,17 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
   wt_default_params(&h->p);
   h->stats.frontal_area = 1;
   cudaGetDevice(&h->device);
+  {
+    // The lean kernel prefetches the populations of the warp this many cells
+    // further on in launch order: a third of the cells its resident blocks
+    // (8 per SM) cover, the best of a sweep on B200 (0.15 to 1.2 of them).
+    // WT_PREFETCH_CELLS overrides it (0 turns the prefetch off).
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    const int gx = (nx + wt::STEP_BX - 1) / wt::STEP_BX;
+    h->pf = (long long)sms * 8 * nx / gx / 3;
+    if (const char* e = getenv("WT_PREFETCH_CELLS")) h->pf = std::max(0LL, atoll(e));
+  }
   h->nsegs = (long long)((nx + 31) / 32) * ny * nz;
   const size_t pop = (size_t)n * 19 * h->elem;
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
@@ -668,8 +680,8 @@ int select_path(wt_lattice* h, Path* out) {
     case WT_KERNEL_LEAN:
       if (!lean_ok(h))
         return fail(h, WT_ERR_UNSUPPORTED,
-                    "the lean kernel needs the float32 collision, buffers under 2 GiB, "
-                    "stationary walls and nearest rounding for half storage");
+                    "the lean kernel needs the float32 collision, buffers under 2 GiB "
+                    "and stationary walls");
       path = Path::Lean;
       break;
     case WT_KERNEL_AUTO:
@@ -1019,12 +1031,15 @@ int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_ad
   const int* b = h->sbox;
   const size_t nbox = (size_t)(b[3] - b[0]) * (b[4] - b[1]) * (b[5] - b[2]);
   AdjBuffers mem;
-  S* cps = (S*)mem.get(pop * (size_t)ncp);          // checkpoints S^{kC}
-  S* seg = (S*)mem.get(pop * (size_t)C);            // states of one segment
+  const size_t pel = pop / sizeof(S);                // elements of one state
+  // checkpoints S^{kC} of every segment but the last, whose states the
+  // forward sweep writes straight into the segment store (C + 1 states)
+  S* cps = ncp > 1 ? (S*)mem.get(pop * (size_t)(ncp - 1)) : nullptr;
+  S* seg = (S*)mem.get(pop * (size_t)(C + 1));
   T* Tbuf[2] = {(T*)mem.get(tsz), (T*)mem.get(tsz)};
   double* ds = (double*)mem.get(sizeof(double) * nbox);
   double* fdev = (double*)mem.get(sizeof(double) * 3 * (size_t)N);
-  if (!cps || !seg || !Tbuf[0] || !Tbuf[1] || !ds || !fdev)
+  if ((ncp > 1 && !cps) || !seg || !Tbuf[0] || !Tbuf[1] || !ds || !fdev)
     return fail(h, WT_ERR_OOM, "cannot allocate the adjoint's checkpoints (" +
                                    std::to_string((pop * (size_t)(ncp + C) + 2 * tsz) >> 20) +
                                    " MiB)");
@@ -1033,37 +1048,62 @@ int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_ad
   cudaEventCreate(&e1);
   cudaEventCreate(&e2);
   WT_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(unsigned), h->stream));
+  const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
+  const bool wide = 19 * h->n >= (1LL << 31);
   cudaEventRecord(e0, h->stream);
   // forward sweep: a checkpoint every C steps, the force series for J
-  for (int k = 0; k < ncp; k++) {
-    WT_CUDA(h, cudaMemcpyAsync(cps + (size_t)k * (pop / sizeof(S)), h->buf[h->parity], pop,
+  for (int k = 0; k + 1 < ncp; k++) {
+    WT_CUDA(h, cudaMemcpyAsync(cps + (size_t)k * pel, h->buf[h->parity], pop,
                                cudaMemcpyDeviceToDevice, h->stream));
-    const int n = std::min(C, N - k * C);
-    dispatch_steps(h, n, Path::Pbb, fdev + 3 * (size_t)k * C);
+    dispatch_steps(h, C, Path::Pbb, fdev + 3 * (size_t)k * C);
+  }
+  const int tl = (ncp - 1) * C, nl = N - tl;   // the last segment
+  {
+    WT_CUDA(h, cudaMemcpyAsync(seg, h->buf[h->parity], pop, cudaMemcpyDeviceToDevice, h->stream));
+    wt::StepArgs<S> fa = make_args<S>(h);
+    const size_t stride = 3 * (size_t)h->nslots;
+    for (int done = 0; done < nl;) {
+      const int chunk = std::min(kChunk, nl - done);
+      for (int s = 0; s < chunk; s++) {
+        fa.F = seg + (size_t)(done + s) * pel;
+        fa.G = seg + (size_t)(done + s + 1) * pel;
+        fa.part = h->part + (size_t)s * stride;
+        fa.write_fields = (done + s == nl - 1) ? 1 : 0;
+        launch_pbb(fa, grid, wide, h->stream);
+        h->launches++;
+      }
+      wt::launch_force_reduce(h->part, (unsigned)h->nslots, chunk,
+                              fdev + 3 * ((size_t)tl + done), h->stream);
+      h->launches++;
+      done += chunk;
+    }
+    WT_CUDA(h, cudaMemcpyAsync(h->buf[h->parity], seg + (size_t)nl * pel, pop,
+                               cudaMemcpyDeviceToDevice, h->stream));
   }
   cudaEventRecord(e1, h->stream);
   // backward sweep, segment by segment: recompute the segment's states from
-  // its checkpoint, then run its adjoint steps last to first
+  // its checkpoint (the last segment's are still in the store), then run its
+  // adjoint steps last to first
   WT_CUDA(h, cudaMemsetAsync(Tbuf[0], 0, tsz, h->stream));
   WT_CUDA(h, cudaMemsetAsync(ds, 0, sizeof(double) * nbox, h->stream));
   int cur = 0;   // Tbuf[cur] holds T^{t+1}
   wt::StepArgs<S> a = make_args<S>(h);
   a.write_fields = 0;
   a.part = h->part;   // force partials of recomputed steps are not reduced
-  const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
-  const bool wide = 19 * h->n >= (1LL << 31);
   for (int k = ncp - 1; k >= 0; k--) {
     const int t0 = k * C, n = std::min(C, N - t0);
-    WT_CUDA(h, cudaMemcpyAsync(seg, cps + (size_t)k * (pop / sizeof(S)), pop,
-                               cudaMemcpyDeviceToDevice, h->stream));
-    for (int j = 0; j + 1 < n; j++) {
-      a.F = seg + (size_t)j * (pop / sizeof(S));
-      a.G = seg + (size_t)(j + 1) * (pop / sizeof(S));
-      launch_pbb(a, grid, wide, h->stream);
-      h->launches++;
+    if (k + 1 < ncp) {
+      WT_CUDA(h, cudaMemcpyAsync(seg, cps + (size_t)k * pel, pop, cudaMemcpyDeviceToDevice,
+                                 h->stream));
+      for (int j = 0; j + 1 < n; j++) {
+        a.F = seg + (size_t)j * pel;
+        a.G = seg + (size_t)(j + 1) * pel;
+        launch_pbb(a, grid, wide, h->stream);
+        h->launches++;
+      }
     }
     for (int t = t0 + n - 1; t >= t0; t--) {
-      a.F = seg + (size_t)(t - t0) * (pop / sizeof(S));
+      a.F = seg + (size_t)(t - t0) * pel;
       const double wJ = t >= N - W ? 1.0 / W : 0.0;
       launch_adj(a, Tbuf[cur], Tbuf[cur ^ 1], ds, wJ, cfg.component, h->stream);
       h->launches++;
@@ -1118,7 +1158,15 @@ extern "C" int wt_adjoint(wt_lattice* h, const wt_adj_cfg* cfg, double* dJds, wt
   if (h->p.kernel != WT_KERNEL_AUTO && h->p.kernel != WT_KERNEL_DIRECT)
     return fail(h, WT_ERR_UNSUPPORTED, "the adjoint runs the direct kernel");
   int C = cfg->checkpoint;
-  if (C == 0) C = std::max(1, (int)std::ceil(std::sqrt((double)cfg->nsteps)));
+  if (C == 0) {
+    // every state when they fit in three quarters of the free memory (no
+    // recomputation), else segments of about sqrt(nsteps) steps
+    size_t freeb = 0, total = 0;
+    WT_CUDA(h, cudaMemGetInfo(&freeb, &total));
+    const size_t pop = (size_t)h->n * 19 * h->elem;
+    if ((double)pop * (cfg->nsteps + 3) <= 0.75 * (double)freeb) C = cfg->nsteps;
+    else C = std::max(1, (int)std::ceil(std::sqrt((double)cfg->nsteps)));
+  }
   C = std::min(C, cfg->nsteps);
   int c = grow_forces(h, 1);
   if (c != WT_OK) return c;

@@ -135,7 +135,21 @@ struct StepArgs {
   S eq[Q];             // equilibrium deviation at rho=1, u=(u0,0,0), rounded to S
   const double* sfrac; // partial bounce-back: solid fraction on the box sb (x fastest), or null
   int sb[6];           // its half-open box x0, y0, z0, x1, y1, z1
+  long long pf;        // L2 prefetch distance in cells (0: none), see prefetch_ahead
 };
+
+// Ask L2 for the populations that the warp pf cells further on in launch
+// order will pull: lane q < 19 prefetches the line holding the first of that
+// warp's 32 pulled values of direction q (the warp beside it covers the rest
+// of a line its values straddle). Issued by a warp before its own loads, it
+// keeps DRAM requests in flight for cells whose blocks have not started yet.
+template <class S>
+__device__ __forceinline__ void prefetch_ahead(const StepArgs<S>& a, long long warp_cell0) {
+  const int lane = threadIdx.x & 31;
+  if (a.pf <= 0 || lane >= 19) return;
+  const long long e = warp_cell0 + a.pf + a.src[lane];
+  if (e >= 0 && e < 19 * a.n) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.F + e));
+}
 
 // The four tensor maps of a lattice for the TMA step kernel: loads (box of
 // (tile width + 2 * halo) x tile rows) and stores (box tile width x tile rows)

@@ -15,6 +15,7 @@ struct wt_lattice {
   int nx = 0, ny = 0, nz = 0, storage = 0;
   long long n = 0;
   int device = 0;
+  long long pf = 0;              // L2 prefetch distance of the lean kernel (cells)
   size_t elem = 4;               // bytes per stored population
   cudaStream_t stream = nullptr;
   void* buf[2] = {nullptr, nullptr};  // population buffers A and B (js/lbm.js:74-75)

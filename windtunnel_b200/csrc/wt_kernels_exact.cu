@@ -34,14 +34,12 @@ void launch_pbb_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cudaS
 
 void launch_adj_f32x(const StepArgs<float>& a, const double* Tn, double* Tc, double* ds,
                      double wJ, int comp, cudaStream_t s) {
-  AdjArgs<double> j{Tn, Tc, ds, wJ, comp};
-  k_adjoint<float, double><<<step_grid(a.nx, a.ny, a.nz), STEP_BX, 0, s>>>(a, j);
+  launch_adjoint<float, double>(a, Tn, Tc, ds, wJ, comp, s);
 }
 
 void launch_adj_f64(const StepArgs<double>& a, const double* Tn, double* Tc, double* ds,
                     double wJ, int comp, cudaStream_t s) {
-  AdjArgs<double> j{Tn, Tc, ds, wJ, comp};
-  k_adjoint<double, double><<<step_grid(a.nx, a.ny, a.nz), STEP_BX, 0, s>>>(a, j);
+  launch_adjoint<double, double>(a, Tn, Tc, ds, wJ, comp, s);
 }
 
 void launch_staged_f32_exact(const StepArgs<float>& a, cudaStream_t s) {

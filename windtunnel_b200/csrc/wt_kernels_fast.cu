@@ -70,14 +70,12 @@ void launch_pbb_f16_fast(const StepArgs<__half>& a, dim3 grid, bool wide, cudaSt
 
 void launch_adj_f32(const StepArgs<float>& a, const float* Tn, float* Tc, double* ds, double wJ,
                     int comp, cudaStream_t s) {
-  AdjArgs<float> j{Tn, Tc, ds, wJ, comp};
-  k_adjoint<float, float><<<step_grid(a.nx, a.ny, a.nz), STEP_BX, 0, s>>>(a, j);
+  launch_adjoint<float, float>(a, Tn, Tc, ds, wJ, comp, s);
 }
 
 void launch_adj_f16(const StepArgs<__half>& a, const float* Tn, float* Tc, double* ds, double wJ,
                     int comp, cudaStream_t s) {
-  AdjArgs<float> j{Tn, Tc, ds, wJ, comp};
-  k_adjoint<__half, float><<<step_grid(a.nx, a.ny, a.nz), STEP_BX, 0, s>>>(a, j);
+  launch_adjoint<__half, float>(a, Tn, Tc, ds, wJ, comp, s);
 }
 
 // ---- TMA tile kernel ------------------------------------------------------------

@@ -10,7 +10,8 @@
 // one add, instead of a 64-bit multiply-add chain per access. Used when both
 // population buffers span less than 2^31 bytes. The outlet column is computed
 // by its own threads (a recomputation of column nx-2), so the common path has
-// no second store per population.
+// no second store per population. Half storage rounds to nearest or
+// stochastically (StepArgs f16_sr), as the direct kernel does.
 #pragma once
 
 #include "wt_x2.cuh"
@@ -23,6 +24,7 @@ __global__ void __launch_bounds__(STEP_BX, 8) k_step_lean(const __grid_constant_
   constexpr float SC = T::SC;
   const int x = blockIdx.x * STEP_BX + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
+  prefetch_ahead(a, (long long)(x - (int)(threadIdx.x & 31)) + (long long)a.nx * y + a.nxy * z);
   double Fx = 0, Fy = 0, Fz = 0;
   bool near_cell = false;
   if (x < a.nx) {
@@ -63,8 +65,30 @@ __global__ void __launch_bounds__(STEP_BX, 8) k_step_lean(const __grid_constant_
       } else if (a.mov && near_cell) {
         a.rho[is] = r * (1.0f / SC);
       }
+      bool stored = false;
+      if constexpr (std::is_same<S, __half>::value) {
+        if (a.f16_sr) {
+          // stochastic rounding, pairs converted together with the direct
+          // kernel's per-cell, per-step random chain (seeded by the computed
+          // cell, so the outlet copy rounds as column nx-2 does)
+          uint32_t h = ((uint32_t)is ^ (uint32_t)(is >> 32)) * 0x9E3779B1u ^ a.sr_seed;
+          h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
 #pragma unroll
-      for (int q = 0; q < Q; q++) gs(q) = T::to_s(f[q]);
+          for (int k = 1; k < Q; k += 2) {
+            h ^= h << 13; h ^= h >> 17; h ^= h << 5;
+            const __half2 p = sr_half2(f[k], f[k + 1], h);
+            gs(k) = __high2half(p);
+            gs(k + 1) = __low2half(p);
+          }
+          h ^= h << 13; h ^= h >> 17; h ^= h << 5;
+          gs(0) = __low2half(sr_half2(0.0f, f[0], h));
+          stored = true;
+        }
+      }
+      if (!stored) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) gs(q) = T::to_s(f[q]);
+      }
     } else if (cat == CAT_EQ) {
 #pragma unroll
       for (int q = 0; q < Q; q++) gs(q) = a.eq[q];

@@ -33,6 +33,20 @@
 
 namespace wt {
 
+// Division and square root of the collision and its adjoint: IEEE in float64
+// (the exact forms), the hardware approximations (relative error ~2^-22) in
+// float32, where the fast forms already use them.
+template <class T>
+__device__ __forceinline__ T cdiv(T n, T d) {
+  if constexpr (std::is_same<T, float>::value) return n * rcp_approx(d);
+  else return n / d;
+}
+template <class T>
+__device__ __forceinline__ T csqrt(T v) {
+  if constexpr (std::is_same<T, float>::value) return sqrt_approx(v);
+  else return sqrt(v);
+}
+
 // Forward collision of one cell and the intermediates its adjoint needs, in
 // the operation order of js/lbm.js:377-460 (and of collide_exact).
 template <class T>
@@ -48,7 +62,7 @@ __device__ __forceinline__ void cell_fw(const StepArgs<S>& a, CellFw<T>& c) {
   const T dr = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] + f[11] +
                f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
   const T r = (T)1 + dr;
-  const T inv = (T)1 / r;
+  const T inv = cdiv((T)1, r);
   const T jx = f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[11] - f[12] + f[13] - f[14];
   const T jy = f[3] - f[4] + f[7] - f[8] - f[9] + f[10] + f[15] - f[16] + f[17] - f[18];
   const T jz = f[5] - f[6] + f[11] - f[12] - f[13] + f[14] + f[15] - f[16] - f[17] + f[18];
@@ -67,7 +81,7 @@ __device__ __forceinline__ void cell_fw(const StepArgs<S>& a, CellFw<T>& c) {
   for (int q = 0; q < Q; q++) c.n[q] = f[q] - e[q];
   const T* n = c.n;
   const T tau0 = (T)a.tau0;
-  T om = (T)1 / tau0, tauEff = tau0;
+  T om = cdiv((T)1, tau0), tauEff = tau0;
   c.pxx = c.pyy = c.pzz = c.pxy = c.pxz = c.pyz = c.mag = c.R = (T)0;
   if (a.les) {
     c.pxx = n[1] + n[2] + n[7] + n[8] + n[9] + n[10] + n[11] + n[12] + n[13] + n[14];
@@ -76,14 +90,14 @@ __device__ __forceinline__ void cell_fw(const StepArgs<S>& a, CellFw<T>& c) {
     c.pxy = n[7] + n[8] - n[9] - n[10];
     c.pxz = n[11] + n[12] - n[13] - n[14];
     c.pyz = n[15] + n[16] - n[17] - n[18];
-    c.mag = sqrt((T)2 * (c.pxx * c.pxx + c.pyy * c.pyy + c.pzz * c.pzz +
-                         (T)2 * (c.pxy * c.pxy + c.pxz * c.pxz + c.pyz * c.pyz)));
+    c.mag = csqrt((T)2 * (c.pxx * c.pxx + c.pyy * c.pyy + c.pzz * c.pzz +
+                          (T)2 * (c.pxy * c.pxy + c.pxz * c.pxz + c.pyz * c.pyz)));
     const T SQ18 = (T)(18 * 1.4142135623730951);
-    c.R = sqrt(tau0 * tau0 + SQ18 * (T)a.cs2 * c.mag * inv);
+    c.R = csqrt(tau0 * tau0 + SQ18 * (T)a.cs2 * c.mag * inv);
     tauEff = (T)0.5 * (tau0 + c.R);
-    om = (T)1 / tauEff;
+    om = cdiv((T)1, tauEff);
   }
-  const T omm = a.trt ? (T)1 / ((T)0.5 + (T)a.lam / (tauEff - (T)0.5)) : om;
+  const T omm = a.trt ? cdiv((T)1, (T)0.5 + cdiv((T)a.lam, tauEff - (T)0.5)) : om;
   c.gc[0] = f[0] - om * (f[0] - e[0]);
 #pragma unroll
   for (int k = 1; k < Q; k += 2) {
@@ -121,16 +135,16 @@ __device__ __forceinline__ void cell_vjp(const StepArgs<S>& a, const CellFw<T>& 
     T teb;
     if (a.trt) {
       const T tm = c.tauEff - (T)0.5;
-      teb = ommb * (c.omm * c.omm * (T)a.lam / (tm * tm)) - omb * (c.om * c.om);
+      teb = ommb * cdiv(c.omm * c.omm * (T)a.lam, tm * tm) - omb * (c.om * c.om);
     } else {
       teb = -(omb + ommb) * (c.om * c.om);
     }
     const T Rb = (T)0.5 * teb;
-    const T Xb = Rb / ((T)2 * c.R);
+    const T Xb = cdiv(Rb, (T)2 * c.R);
     const T K = (T)(18 * 1.4142135623730951) * (T)a.cs2;
     const T magb = Xb * K * c.inv;
     invb += Xb * K * c.mag;
-    const T Qb = c.mag > (T)0 ? magb / c.mag : (T)0;
+    const T Qb = c.mag > (T)0 ? cdiv(magb, c.mag) : (T)0;
     const T pxxb = (T)2 * c.pxx * Qb, pyyb = (T)2 * c.pyy * Qb, pzzb = (T)2 * c.pzz * Qb;
     const T pxyb = (T)4 * c.pxy * Qb, pxzb = (T)4 * c.pxz * Qb, pyzb = (T)4 * c.pyz * Qb;
     nb[1] += pxxb; nb[2] += pxxb;
@@ -287,105 +301,194 @@ struct AdjArgs {
   double* ds;      // dJ/ds accumulated on the solid-fraction box
   double wJ;       // weight of this step's force in J
   int comp;        // force component of J
+  long long gat[Q];   // element offset from cell i to its link-q consumer: q*n + ex + nx ey + nxy ez
+  int gatb[Q];        // gat[q] * sizeof(T), when every offset fits in 31 bits
+  int rowb[Q];        // q*n * sizeof(T), likewise
 };
 
-// Adjoint of the population stored at (q, location lx,ly,lz) after a step:
-// the sum of Tn over the links that pull it next step. loc_near: the
-// location is a computed near-wall cell whose neighbour bits are in m.
+// The free-slip term of the adjoint of the population stored at (q, location
+// lx,ly,lz): when the location's link-q consumer lies on a side plane y or z,
+// the cell mirrored back into the interior pulls it through the mirrored link.
 template <class T, class S>
-__device__ __forceinline__ T adj_gather(const StepArgs<S>& a, const T* Tn, int q, int lx, int ly,
-                                        int lz, unsigned long long m) {
+__device__ __forceinline__ T adj_mirror(const StepArgs<S>& a, const T* Tn, int q, int lx, int ly,
+                                        int lz) {
   const int px = lx + ex(q), py = ly + ey(q), pz = lz + ez(q);
-  T v = (T)0;
-  if (px >= 0 && px < a.nx) v = Tn[(long long)q * a.n + px + (long long)a.nx * py + a.nxy * pz];
-  if ((m >> opp(q)) & 1ull)   // neighbour (px,py,pz) is solid: the location's own cell bounces it
-    v += Tn[(long long)opp(q) * a.n + lx + (long long)a.nx * ly + a.nxy * lz];
-  if (a.freeslip) {
-    const bool ym = py == 0 || py == a.ny - 1, zm = pz == 0 || pz == a.nz - 1;
-    if (ym || zm) {
-      const int sy = ym ? py : ly, sz = zm ? pz : lz;
-      if (!(a.flags[lx + (long long)a.nx * sy + a.nxy * sz] & FLAG_SOLID_MASK) && px >= 0 &&
-          px < a.nx) {
-        const int cy = ym ? ly : py, cz = zm ? lz : pz;
-        int qq = q;
-        if (ym) qq = mirror_y(qq);
-        if (zm) qq = mirror_z(qq);
-        v += Tn[(long long)qq * a.n + px + (long long)a.nx * cy + a.nxy * cz];
-      }
-    }
-  }
+  const bool ym = py == 0 || py == a.ny - 1, zm = pz == 0 || pz == a.nz - 1;
+  if (!(ym || zm) || px < 0 || px >= a.nx) return (T)0;
+  const int sy = ym ? py : ly, sz = zm ? pz : lz;
+  if (a.flags[lx + (long long)a.nx * sy + a.nxy * sz] & FLAG_SOLID_MASK) return (T)0;
+  const int cy = ym ? ly : py, cz = zm ? lz : pz;
+  int qq = q;
+  if (ym) qq = mirror_y(qq);
+  if (zm) qq = mirror_z(qq);
+  return Tn[(long long)qq * a.n + px + (long long)a.nx * cy + a.nxy * cz];
+}
+
+// The free-slip terms of a shell cell's gathered adjoint of link q: the
+// mirrors of its own consumer and, at x = nx-2, those of the outlet column's
+// copy of the cell.
+template <class T, class S>
+__device__ __forceinline__ T adj_shell(const StepArgs<S>& a, const T* Tn, int q, int x, int y,
+                                       int z) {
+  T v = adj_mirror<T>(a, Tn, q, x, y, z);
+  if (x == a.nx - 2) v += adj_mirror<T>(a, Tn, q, x + 1, y, z);
   return v;
 }
 
-template <class S, class T>
-__global__ void __launch_bounds__(STEP_BX) k_adjoint(const __grid_constant__ StepArgs<S> a,
-                                                      const __grid_constant__ AdjArgs<T> j) {
+// One adjoint step, one thread per cell. A computed cell recomputes its
+// forward collision from the stored state, gathers the adjoints of the 19
+// populations it stored (the consumers of its links in the next step), runs
+// the collision's vector-Jacobian product and writes the adjoints of the 19
+// values it pulled; cells of the solid-fraction box also accumulate dJ/ds.
+// NB: offsets in bytes (every buffer spans < 2^31 bytes) instead of 64-bit
+// element indices.
+// Resident blocks per SM the register budget is set for: float32 adjoints
+// fit 96 registers without spilling (20 warps per SM); float64 ones take 168.
+template <class T>
+constexpr int adj_min_blocks() { return sizeof(T) == 4 ? 5 : 3; }
+
+template <class S, class T, bool NB>
+__global__ void __launch_bounds__(STEP_BX, adj_min_blocks<T>()) k_adjoint(const __grid_constant__ StepArgs<S> a,
+                                                         const __grid_constant__ AdjArgs<T> j) {
   const int x = blockIdx.x * STEP_BX + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
-  if (x >= a.nx) return;
   const long long i = (long long)x + (long long)a.nx * y + a.nxy * z;
+  if (x >= a.nx) return;
   const uint8_t fl = a.flags[i];
   const bool computed = x >= 1 && x <= a.nx - 2 && y >= 1 && y <= a.ny - 2 && z >= 1 &&
                         z <= a.nz - 2 && !(fl & FLAG_SOLID_MASK);
   T* Tci = j.Tc + i;
+  const T* Tni = j.Tn + i;
+  const S* Fi = a.F + i;
+  auto trow = [&](T* p, int q) -> T& {
+    if constexpr (NB) return *reinterpret_cast<T*>(reinterpret_cast<char*>(p) + j.rowb[q]);
+    else return p[a.dst[q]];
+  };
   if (!computed) {
 #pragma unroll
-    for (int q = 0; q < Q; q++) Tci[(long long)q * a.n] = (T)0;
+    for (int q = 0; q < Q; q++) trow(Tci, q) = (T)0;
     return;
   }
-  const unsigned long long m = (fl & FLAG_NEAR) ? a.nmask[i] : 0ull;
-  T gb[Q];
-#pragma unroll
-  for (int q = 0; q < Q; q++) {
-    gb[q] = adj_gather<T>(a, j.Tn, q, x, y, z, m);
-    if (x == a.nx - 2) gb[q] += adj_gather<T>(a, j.Tn, q, x + 1, y, z, 0ull);   // outlet copy
-  }
-  // pulled populations (stationary walls) and the body links
-  CellFw<T> c;
+  auto tn_row = [&](int q) -> T {
+    if constexpr (NB) return *reinterpret_cast<const T*>(reinterpret_cast<const char*>(Tni) + j.rowb[q]);
+    else return Tni[a.dst[q]];
+  };
+  auto tn_gat = [&](int q) -> T {
+    if constexpr (NB) return *reinterpret_cast<const T*>(reinterpret_cast<const char*>(Tni) + j.gatb[q]);
+    else return Tni[j.gat[q]];
+  };
+  auto tn_gat1 = [&](int q) -> T {   // the consumer of cell i+1's link q
+    if constexpr (NB) return *reinterpret_cast<const T*>(reinterpret_cast<const char*>(Tni + 1) + j.gatb[q]);
+    else return Tni[j.gat[q] + 1];
+  };
+  auto f_pull = [&](int q) -> T {
+    if constexpr (NB) return (T)ld<T>(*reinterpret_cast<const S*>(reinterpret_cast<const char*>(Fi) + a.srcb[q]));
+    else return (T)ld<T>(Fi[a.src[q]]);
+  };
+  auto f_own = [&](int q) -> T {
+    if constexpr (NB) return (T)ld<T>(*reinterpret_cast<const S*>(reinterpret_cast<const char*>(Fi) + a.dstb[q]));
+    else return (T)ld<T>(Fi[a.dst[q]]);
+  };
+  // The free-slip mirror terms of shell cells go first, while few values are
+  // live, into this thread's column of shared memory.
+  __shared__ T mir[Q][STEP_BX];
   const bool shell = a.freeslip && (y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2);
+  if (shell) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) mir[q][threadIdx.x] = adj_shell<T>(a, j.Tn, q, x, y, z);
+  }
+  const unsigned long long m = (fl & FLAG_NEAR) ? a.nmask[i] : 0ull;
   const unsigned sm = (unsigned)m, om = (unsigned)(m >> 32);
+  // gathered adjoints of the stored populations: the plain consumer, plus the
+  // cell itself where the link's neighbour is solid (it bounces the value),
+  // plus at x = nx-2 the consumer of the outlet column's copy (x+1 + c_q,
+  // inside the lattice when c_q has no +x component)
+  T g[Q];
 #pragma unroll
   for (int q = 0; q < Q; q++) {
-    if ((sm >> q) & 1u) {
-      c.f[q] = (T)ld<T>(a.F[opp(q) * a.n + i]);
-    } else if (shell) {
-      int sy = y - ey(q), sz = z - ez(q), qq = q;
-      if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); }
-      if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); }
-      c.f[q] = (T)ld<T>(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);
-    } else {
-      c.f[q] = (T)ld<T>(a.F[a.src[q] + i]);
+    g[q] = tn_gat(q);
+    if ((sm >> opp(q)) & 1u) g[q] += tn_row(opp(q));
+  }
+  if (x == a.nx - 2) {
+#pragma unroll
+    for (int q = 0; q < Q; q++)
+      if (ex(q) <= 0) g[q] += tn_gat1(q);
+  }
+  if (shell) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) g[q] += mir[q][threadIdx.x];
+  }
+  // pulled populations (stationary walls) and the forward collision
+  CellFw<T> c;
+  if (!shell) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) c.f[q] = ((sm >> q) & 1u) ? f_own(opp(q)) : f_pull(q);
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      if ((sm >> q) & 1u) {
+        c.f[q] = f_own(opp(q));
+      } else {
+        int sy = y - ey(q), sz = z - ez(q), qq = q;
+        if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); }
+        if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); }
+        c.f[q] = (T)ld<T>(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);
+      }
     }
   }
   cell_fw<T>(a, c);
-  const double s = sfrac_at(a, x, y, z);
-  const T st = (T)s, wJ = (T)j.wJ;
-  T ab[Q], fb[Q];
-#pragma unroll
-  for (int q = 0; q < Q; q++) {
-    const T cc = (T)(j.comp == 0 ? ex(q) : (j.comp == 1 ? ey(q) : ez(q)));
-    ab[q] = ((T)1 - st) * gb[q] + wJ * st * cc;
-    fb[q] = st * gb[opp(q)] + wJ * st * cc;
-    if ((om >> q) & 1u) fb[q] -= (T)2 * wJ * cc;
-  }
+  const T wJ = (T)j.wJ;
+  // partial bounce-back: g = (1-s) gc + s f_opp, force s sum_q c_q (gc_q - f_opp(q))
+  T st = (T)0;
   if (a.sfrac && x >= a.sb[0] && x < a.sb[3] && y >= a.sb[1] && y < a.sb[4] && z >= a.sb[2] &&
       z < a.sb[5]) {
-    // dJ/ds = sum_q gb_q (f_opp(q) - gc_q) + wJ sum_q c_q (gc_q - f_opp(q))
+    st = (T)sfrac_at(a, x, y, z);
+    // dJ/ds = sum_q g_q (f_opp(q) - gc_q) + wJ sum_q c_q (gc_q - f_opp(q))
     T g1 = (T)0, g2 = (T)0;
 #pragma unroll
     for (int q = 0; q < Q; q++) {
       const T cc = (T)(j.comp == 0 ? ex(q) : (j.comp == 1 ? ey(q) : ez(q)));
       const T d = c.f[opp(q)] - c.gc[q];
-      g1 += gb[q] * d;
+      g1 += g[q] * d;
       g2 -= cc * d;
     }
     j.ds[(x - a.sb[0]) + (long long)(a.sb[3] - a.sb[0]) *
                              ((y - a.sb[1]) + (long long)(a.sb[4] - a.sb[1]) * (z - a.sb[2]))] +=
         (double)(g1 + wJ * g2);
   }
+  // adjoints of the collided values (ab) and, through the blend and the
+  // force, of the pulled ones (fb); st = 0 leaves ab = g, fb = 0
+  T ab[Q], fb[Q];
+  const T ws = wJ * st, s1 = (T)1 - st;
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    const T cc = (T)(j.comp == 0 ? ex(q) : (j.comp == 1 ? ey(q) : ez(q)));
+    ab[q] = s1 * g[q] + ws * cc;
+    fb[q] = st * g[opp(q)] + ws * cc;
+    if ((om >> q) & 1u) fb[q] -= (T)2 * wJ * cc;   // momentum exchange of a body link
+  }
   cell_vjp<T>(a, c, ab, fb);
 #pragma unroll
-  for (int q = 0; q < Q; q++) Tci[(long long)q * a.n] = fb[q];
+  for (int q = 0; q < Q; q++) trow(Tci, q) = fb[q];
+}
+
+// Launch one adjoint step (both kernels' offset forms are instantiated by the
+// translation unit that calls this).
+template <class S, class T>
+inline void launch_adjoint(const StepArgs<S>& a, const T* Tn, T* Tc, double* ds, double wJ,
+                           int comp, cudaStream_t s) {
+  AdjArgs<T> j{};
+  j.Tn = Tn; j.Tc = Tc; j.ds = ds; j.wJ = wJ; j.comp = comp;
+  const size_t wide_elem = sizeof(S) > sizeof(T) ? sizeof(S) : sizeof(T);
+  const bool nb = 19 * a.n * (long long)wide_elem < (1LL << 31);
+  for (int q = 0; q < Q; q++) {
+    j.gat[q] = q * a.n + ex(q) + (long long)a.nx * ey(q) + a.nxy * ez(q);
+    j.gatb[q] = nb ? (int)(j.gat[q] * (long long)sizeof(T)) : 0;
+    j.rowb[q] = nb ? (int)(q * a.n * (long long)sizeof(T)) : 0;
+  }
+  const dim3 grid = step_grid(a.nx, a.ny, a.nz);
+  if (nb) k_adjoint<S, T, true><<<grid, STEP_BX, 0, s>>>(a, j);
+  else k_adjoint<S, T, false><<<grid, STEP_BX, 0, s>>>(a, j);
 }
 
 }  // namespace wt

@@ -144,6 +144,19 @@ __device__ __forceinline__ void patch_special(const StepArgs<S>& a, long long i,
 #undef WT_PATCH
 }
 
+// Hardware approximations (relative error ~2^-22) used by the float32
+// collisions: one instruction each instead of a correctly rounded sequence.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Float32 collision, re-associated: opposite pairs are carried as half sums
 // and half differences, so moments, the equilibrium, the stress tensor of the
 // Smagorinsky model and the TRT update share their partial results. The
@@ -164,7 +177,11 @@ __device__ __forceinline__ void collide_fast(const StepArgs<S>& a, const float (
   const float dr = ((f[0] + s1) + (s3 + s5)) + ((s7 + s9) + (s11 + s13)) + (s15 + s17);
   const float r = 1.0f + dr;
   if (!(r > 0.0f && r < 3.0e38f)) atomicOr(a.err, 1u);
-  const float inv = __frcp_rn(r);
+  // Half storage takes the one-instruction approximations (its step is
+  // issue-bound); float32 keeps the correctly rounded forms, which measured
+  // faster there (the approximations' register allocation spills at 64).
+  constexpr bool APPROX = std::is_same<S, __half>::value;
+  const float inv = APPROX ? rcp_approx(r) : __frcp_rn(r);
   const float vx = ((d1 + d7) + (d9 + d11) + d13) * inv;
   const float vy = ((d3 + d7) - d9 + (d15 + d17)) * inv;
   const float vz = ((d5 + d11) - d13 + (d15 - d17)) * inv;
@@ -199,8 +216,10 @@ __device__ __forceinline__ void collide_fast(const StepArgs<S>& a, const float (
     const float qq = sxx * sxx + syy * syy + szz * szz + 2.0f * (sxy * sxy + sxz * sxz + syz * syz);
     // SQ18 * cs2 * |Pi| / r with |Pi| = 2 sqrt(2 qq): 72 cs2 sqrt(qq) / r
     const float tau0 = a.tau0f;
-    const float te = 0.5f * (tau0 + sqrtf(fmaf(tau0, tau0, a.les_cf * sqrtf(qq) * inv)));
-    om = __frcp_rn(te);
+    const float te =
+        APPROX ? 0.5f * (tau0 + sqrt_approx(fmaf(tau0, tau0, a.les_cf * sqrt_approx(qq) * inv)))
+               : 0.5f * (tau0 + sqrtf(fmaf(tau0, tau0, a.les_cf * sqrtf(qq) * inv)));
+    om = APPROX ? rcp_approx(te) : __frcp_rn(te);
     if (a.trt) {
       const float t5 = te - 0.5f;
       omm = __fdividef(t5, fmaf(0.5f, t5, a.lamf));

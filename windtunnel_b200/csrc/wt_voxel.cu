@@ -13,10 +13,11 @@
 //                    (u, v) sample rows and mark the shell cells
 //   k_vox_ranges     per triangle its bucket rectangle in the plane normal to
 //                    the ray axis (48 x 48 buckets at most, js/voxel.js:151-171)
-//   k_vox_bucket     one thread per bucket walks the triangles in index order,
-//                    counting (pass 0) or listing (pass 1) its members, so each
-//                    bucket lists its triangles in the reference's order; an
-//                    exclusive scan of the counts runs in between (k_vox_scan)
+//   k_vox_bucket     one warp per bucket walks the triangles in index order,
+//                    32 at a time, counting (pass 0) or listing (pass 1) its
+//                    members with ballot ranks, so each bucket lists its
+//                    triangles in the reference's order; an exclusive scan of
+//                    the counts runs in between (k_vox_scan)
 //   k_vox_rays       one thread per ray (column): gathers the crossings of its
 //                    bucket's triangles (at most 512, as the reference), sorts
 //                    them, and adds a vote to the cells between alternate pairs
@@ -113,21 +114,29 @@ __global__ void k_vox_ranges(const float* __restrict__ P, long long ntri, AxisGe
 }
 
 // pass 0: count[b] = members of bucket b; pass 1: items[start[b] ...] in
-// triangle order.
+// triangle order. One warp per bucket: the lanes test 32 consecutive
+// triangles at a time and a ballot gives each member its rank, so the list
+// keeps the reference's order.
 __global__ void k_vox_bucket(const int4* __restrict__ rect, long long ntri, int nbB, int nb,
                              int pass, int* __restrict__ count, const int* __restrict__ start,
                              int* __restrict__ items) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nb) return;
+  const int b = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (b >= nb) return;   // whole warps leave together
   const int bb = b % nbB, cc = b / nbB;
   int k = pass ? start[b] : 0;
-  for (long long t = 0; t < ntri; t++) {
-    const int4 r = rect[t];
-    if (bb < r.x || bb > r.y || cc < r.z || cc > r.w) continue;
-    if (pass) items[k] = (int)t;
-    k++;
+  for (long long t0 = 0; t0 < ntri; t0 += 32) {
+    const long long t = t0 + lane;
+    bool hit = false;
+    if (t < ntri) {
+      const int4 r = rect[t];
+      hit = bb >= r.x && bb <= r.y && cc >= r.z && cc <= r.w;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    if (pass && hit) items[k + __popc(m & ((1u << lane) - 1u))] = (int)t;
+    k += __popc(m);
   }
-  if (!pass) count[b] = k;
+  if (!pass && lane == 0) count[b] = k;
 }
 
 // Exclusive scan of nb counts (one block; nb <= 48*48).
@@ -340,8 +349,8 @@ int wt_voxel_build(const float* tris, int64_t ntri, int res, uint8_t* grid, size
     const int nb = x.nbB * x.nbC;
     k_vox_ranges<<<(unsigned)std::min<long long>((ntri + 255) / 256, 4096), 256, 0, s>>>(
         P, ntri, x, rect);
-    k_vox_bucket<<<(nb + 127) / 128, 128, 0, s>>>(rect, ntri, x.nbB, nb, 0, bcount, nullptr,
-                                                   nullptr);
+    k_vox_bucket<<<(nb * 32 + 127) / 128, 128, 0, s>>>(rect, ntri, x.nbB, nb, 0, bcount,
+                                                        nullptr, nullptr);
     k_vox_scan<<<1, 32, 0, s>>>(bcount, nb, bstart);
     int total = 0;
     cudaMemcpyAsync(&total, bstart + nb, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -349,8 +358,8 @@ int wt_voxel_build(const float* tris, int64_t ntri, int res, uint8_t* grid, size
     VoxBuffers items_mem;
     int* items = (int*)items_mem.get(sizeof(int) * (size_t)(total > 0 ? total : 1));
     if (!items) return done(WT_ERR_OOM, "cannot allocate the bucket lists");
-    k_vox_bucket<<<(nb + 127) / 128, 128, 0, s>>>(rect, ntri, x.nbB, nb, 1, nullptr, bstart,
-                                                   items);
+    k_vox_bucket<<<(nb * 32 + 127) / 128, 128, 0, s>>>(rect, ntri, x.nbB, nb, 1, nullptr,
+                                                        bstart, items);
     const long long cols = (long long)x.nB * x.nC;
     k_vox_rays<<<(unsigned)((cols + 127) / 128), 128, 0, s>>>(P, bstart, items, x, votes,
                                                               scratch);

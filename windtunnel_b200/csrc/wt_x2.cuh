@@ -53,16 +53,6 @@ __device__ __forceinline__ f2 psub(f2 a, f2 b) {
   memcpy(&d, &rd, 8);
   return d;
 }
-__device__ __forceinline__ float rcp_approx(float x) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ float sqrt_approx(float x) {
-  float y;
-  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
 __device__ __forceinline__ f2 prcp(f2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
 __device__ __forceinline__ f2 psqrt(f2 a) { return make_float2(sqrt_approx(a.x), sqrt_approx(a.y)); }
 

@@ -19,6 +19,7 @@ import math
 
 from .lbm import LBM
 from .shapes import Body
+from .stats import block_stats
 
 NX, NY, NZ, WARM, AVG = 96, 44, 44, 400, 300
 TAU = 0.5 + math.pow(10, -1.1 - 2.3 * 0.62)
@@ -52,8 +53,9 @@ def run_case(name: str, key: str, ground: bool, aoa: float, storage: str = "f32"
     sim.step_forces(WARM)
     F = sim.step_forces(AVG)
     q = 0.5 * sim.u0 * sim.u0 * area
+    sem = block_stats(F[:, 0] / q).sem   # blocking standard error of the mean drag
     out = {"case": name, "cd": float(F[:, 0].mean() / q), "cl": float(F[:, 1].mean() / q),
-           "solid_cells": sim.solidCells, "area": area,
+           "cd_sem": float(sem), "solid_cells": sim.solidCells, "area": area,
            "area_kind": "planform" if b.ref == "planform" else "frontal"}
     out["published"] = PUBLISHED.get(name, {})
     sim.close()
