@@ -405,9 +405,11 @@ __global__ void __launch_bounds__(STEP_BX, adj_min_blocks<T>()) k_adjoint(const 
   // inside the lattice when c_q has no +x component)
   T g[Q];
 #pragma unroll
-  for (int q = 0; q < Q; q++) {
-    g[q] = tn_gat(q);
-    if ((sm >> opp(q)) & 1u) g[q] += tn_row(opp(q));
+  for (int q = 0; q < Q; q++) g[q] = tn_gat(q);
+  if (sm) {
+#pragma unroll
+    for (int q = 0; q < Q; q++)
+      if ((sm >> opp(q)) & 1u) g[q] += tn_row(opp(q));
   }
   if (x == a.nx - 2) {
 #pragma unroll
@@ -418,23 +420,25 @@ __global__ void __launch_bounds__(STEP_BX, adj_min_blocks<T>()) k_adjoint(const 
 #pragma unroll
     for (int q = 0; q < Q; q++) g[q] += mir[q][threadIdx.x];
   }
-  // pulled populations (stationary walls) and the forward collision
+  // pulled populations (stationary walls: a solid neighbour's link takes the
+  // cell's own opposite population) and the forward collision
   CellFw<T> c;
   if (!shell) {
 #pragma unroll
-    for (int q = 0; q < Q; q++) c.f[q] = ((sm >> q) & 1u) ? f_own(opp(q)) : f_pull(q);
+    for (int q = 0; q < Q; q++) c.f[q] = f_pull(q);
   } else {
 #pragma unroll
     for (int q = 0; q < Q; q++) {
-      if ((sm >> q) & 1u) {
-        c.f[q] = f_own(opp(q));
-      } else {
-        int sy = y - ey(q), sz = z - ez(q), qq = q;
-        if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); }
-        if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); }
-        c.f[q] = (T)ld<T>(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);
-      }
+      int sy = y - ey(q), sz = z - ez(q), qq = q;
+      if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); }
+      if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); }
+      c.f[q] = (T)ld<T>(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);
     }
+  }
+  if (sm) {
+#pragma unroll
+    for (int q = 0; q < Q; q++)
+      if ((sm >> q) & 1u) c.f[q] = f_own(opp(q));
   }
   cell_fw<T>(a, c);
   const T wJ = (T)j.wJ;
@@ -457,15 +461,29 @@ __global__ void __launch_bounds__(STEP_BX, adj_min_blocks<T>()) k_adjoint(const 
         (double)(g1 + wJ * g2);
   }
   // adjoints of the collided values (ab) and, through the blend and the
-  // force, of the pulled ones (fb); st = 0 leaves ab = g, fb = 0
+  // force, of the pulled ones (fb); s = 0 leaves ab = g, fb = 0
   T ab[Q], fb[Q];
-  const T ws = wJ * st, s1 = (T)1 - st;
+  if (st != (T)0) {
+    const T ws = wJ * st, s1 = (T)1 - st;
 #pragma unroll
-  for (int q = 0; q < Q; q++) {
-    const T cc = (T)(j.comp == 0 ? ex(q) : (j.comp == 1 ? ey(q) : ez(q)));
-    ab[q] = s1 * g[q] + ws * cc;
-    fb[q] = st * g[opp(q)] + ws * cc;
-    if ((om >> q) & 1u) fb[q] -= (T)2 * wJ * cc;   // momentum exchange of a body link
+    for (int q = 0; q < Q; q++) {
+      const T cc = (T)(j.comp == 0 ? ex(q) : (j.comp == 1 ? ey(q) : ez(q)));
+      ab[q] = s1 * g[q] + ws * cc;
+      fb[q] = st * g[opp(q)] + ws * cc;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      ab[q] = g[q];
+      fb[q] = (T)0;
+    }
+  }
+  if (om) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      const T cc = (T)(j.comp == 0 ? ex(q) : (j.comp == 1 ? ey(q) : ez(q)));
+      if ((om >> q) & 1u) fb[q] -= (T)2 * wJ * cc;   // momentum exchange of a body link
+    }
   }
   cell_vjp<T>(a, c, ab, fb);
 #pragma unroll
