@@ -354,9 +354,8 @@ __global__ void __launch_bounds__(STEP_BX, adj_min_blocks<T>()) k_adjoint(const 
   const int y = blockIdx.y, z = blockIdx.z;
   const long long i = (long long)x + (long long)a.nx * y + a.nxy * z;
   if (x >= a.nx) return;
-  const uint8_t fl = a.flags[i];
-  const bool computed = x >= 1 && x <= a.nx - 2 && y >= 1 && y <= a.ny - 2 && z >= 1 &&
-                        z <= a.nz - 2 && !(fl & FLAG_SOLID_MASK);
+  const bool inner = x >= 1 && x <= a.nx - 2 && y >= 1 && y <= a.ny - 2 && z >= 1 &&
+                     z <= a.nz - 2;
   T* Tci = j.Tc + i;
   const T* Tni = j.Tn + i;
   const S* Fi = a.F + i;
@@ -364,7 +363,7 @@ __global__ void __launch_bounds__(STEP_BX, adj_min_blocks<T>()) k_adjoint(const 
     if constexpr (NB) return *reinterpret_cast<T*>(reinterpret_cast<char*>(p) + j.rowb[q]);
     else return p[a.dst[q]];
   };
-  if (!computed) {
+  if (!inner) {
 #pragma unroll
     for (int q = 0; q < Q; q++) trow(Tci, q) = (T)0;
     return;
@@ -397,15 +396,37 @@ __global__ void __launch_bounds__(STEP_BX, adj_min_blocks<T>()) k_adjoint(const 
 #pragma unroll
     for (int q = 0; q < Q; q++) mir[q][threadIdx.x] = adj_shell<T>(a, j.Tn, q, x, y, z);
   }
-  const unsigned long long m = (fl & FLAG_NEAR) ? a.nmask[i] : 0ull;
-  const unsigned sm = (unsigned)m, om = (unsigned)(m >> 32);
-  // gathered adjoints of the stored populations: the plain consumer, plus the
-  // cell itself where the link's neighbour is solid (it bounces the value),
-  // plus at x = nx-2 the consumer of the outlet column's copy (x+1 + c_q,
-  // inside the lattice when c_q has no +x component)
+  // Gathered adjoints of the stored populations (plain consumers) and the
+  // pulled populations, issued before the cell's flags byte arrives: every
+  // source of an inner cell lies inside the lattice.
   T g[Q];
 #pragma unroll
   for (int q = 0; q < Q; q++) g[q] = tn_gat(q);
+  CellFw<T> c;
+  if (!shell) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) c.f[q] = f_pull(q);
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      int sy = y - ey(q), sz = z - ez(q), qq = q;
+      if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); }
+      if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); }
+      c.f[q] = (T)ld<T>(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);
+    }
+  }
+  const uint8_t fl = a.flags[i];
+  if (fl & FLAG_SOLID_MASK) {   // solids do not pull
+#pragma unroll
+    for (int q = 0; q < Q; q++) trow(Tci, q) = (T)0;
+    return;
+  }
+  const unsigned long long m = (fl & FLAG_NEAR) ? a.nmask[i] : 0ull;
+  const unsigned sm = (unsigned)m, om = (unsigned)(m >> 32);
+  // the rest of the gathered adjoints: the cell itself where the link's
+  // neighbour is solid (it bounces the value), at x = nx-2 the consumer of
+  // the outlet column's copy (x+1 + c_q, inside the lattice when c_q has no
+  // +x component), the free-slip mirrors
   if (sm) {
 #pragma unroll
     for (int q = 0; q < Q; q++)
@@ -420,21 +441,8 @@ __global__ void __launch_bounds__(STEP_BX, adj_min_blocks<T>()) k_adjoint(const 
 #pragma unroll
     for (int q = 0; q < Q; q++) g[q] += mir[q][threadIdx.x];
   }
-  // pulled populations (stationary walls: a solid neighbour's link takes the
-  // cell's own opposite population) and the forward collision
-  CellFw<T> c;
-  if (!shell) {
-#pragma unroll
-    for (int q = 0; q < Q; q++) c.f[q] = f_pull(q);
-  } else {
-#pragma unroll
-    for (int q = 0; q < Q; q++) {
-      int sy = y - ey(q), sz = z - ez(q), qq = q;
-      if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); }
-      if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); }
-      c.f[q] = (T)ld<T>(a.F[qq * a.n + (x - ex(q)) + (long long)a.nx * sy + a.nxy * sz]);
-    }
-  }
+  // stationary walls: a solid neighbour's link takes the cell's own opposite
+  // population
   if (sm) {
 #pragma unroll
     for (int q = 0; q < Q; q++)
