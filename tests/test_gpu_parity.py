@@ -307,6 +307,48 @@ def test_lean_stochastic_rounding_agrees_with_direct(both):
     assert np.abs(pa - pb).max() <= 1e-4
 
 
+@pytest.mark.parametrize("dims", [(40, 14, 12), (64, 20, 18), (130, 9, 9), (136, 10, 9)])
+@pytest.mark.parametrize("rounding", ["nearest", "stochastic"])
+@pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
+def test_pair_kernel_bit_identical_to_lean(both, dims, rounding, side_bc):
+    """The half-pair kernel collides each cell as the lean kernel does: the
+    populations, fields and force series are bit-identical, with a body at
+    the outlet column, a road and either side condition, on rows of one,
+    a fraction of and several of its 128-cell blocks."""
+    LBM, _ = both
+    out = []
+    for kern in ("lean", "pair"):
+        s = LBM(*dims, storage="f16dev", kernel=kern, side_bc=side_bc)
+        s.set_params(f16_rounding=rounding)
+        apply_case(s, sphere=(dims[0] - 4.5, dims[1] / 2, dims[2] / 2, 3.3), side_bc=side_bc,
+                   ground=True)
+        f1 = s.step_forces(7)
+        u1 = s.fields()
+        f2 = s.step_forces(18)
+        out.append((np.concatenate([f1, f2]), u1, s.fields(), s.populations("f", "raw"),
+                    s.populations("g", "raw")))
+    (fa, ua1, ua2, pa, ga), (fb, ub1, ub2, pb, gb) = out
+    assert np.array_equal(fa, fb)
+    for a, b in list(zip(ua1, ub1)) + list(zip(ua2, ub2)):
+        assert np.array_equal(a, b)
+    assert np.array_equal(pa, pb)
+    assert np.array_equal(ga, gb)
+
+
+def test_pair_kernel_conditions(both):
+    from windtunnel_b200 import WTError
+    LBM, _ = both
+    for dims, storage in (((41, 12, 10), "f16dev"), ((40, 12, 10), "f32")):
+        s = LBM(*dims, storage=storage, kernel="pair")
+        with pytest.raises(WTError):
+            s.step_forces(1)
+    s = LBM(40, 12, 10, storage="f16dev", kernel="pair")
+    apply_case(s, sphere=(20.0, 6.0, 5.0, 3.0), ground=True, roadVel=0.02)
+    s.set_params(moving_walls=1)
+    with pytest.raises(WTError):
+        s.step_forces(1)
+
+
 @pytest.mark.parametrize("storage", ["f32", "f16dev"])
 def test_lean_prefetch_changes_nothing(both, storage, monkeypatch):
     """The lean kernel's L2 prefetch distance (read at create time) moves

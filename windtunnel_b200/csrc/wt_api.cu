@@ -86,7 +86,7 @@ int check_params(const wt_params* p) {
   if (p->trt && !(p->lambda > 0)) return WT_ERR_ARG;
   if (p->side_bc != WT_SIDE_EQ && p->side_bc != WT_SIDE_FREESLIP) return WT_ERR_ARG;
   if (p->math != WT_MATH_FAST && p->math != WT_MATH_EXACT) return WT_ERR_ARG;
-  if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_LEAN) return WT_ERR_ARG;
+  if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_PAIR) return WT_ERR_ARG;
   if (p->f16_rounding != WT_ROUND_NEAREST && p->f16_rounding != WT_ROUND_STOCHASTIC)
     return WT_ERR_ARG;
   if (p->reserved != 0) return WT_ERR_ARG;
@@ -136,8 +136,8 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
     const long long off = wt::ex(q) + (long long)h->nx * wt::ey(q) + a.nxy * wt::ez(q);
     a.src[q] = q * h->n - off;
     a.dst[q] = q * h->n;
-    a.srcb[q] = narrow ? (int)(a.src[q] * (long long)sizeof(S)) : 0;
-    a.dstb[q] = narrow ? (int)(a.dst[q] * (long long)sizeof(S)) : 0;
+    a.srcb[q] = narrow ? (uint32_t)(a.src[q] * (long long)sizeof(S)) : 0u;
+    a.dstb[q] = narrow ? (uint32_t)(a.dst[q] * (long long)sizeof(S)) : 0u;
   }
   const wt_params& p = h->p;
   a.tau0 = p.tau;
@@ -168,12 +168,13 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
 // direction block starts on a 16-byte boundary.
 bool staged_ok(const wt_lattice* h) { return h->nx % (int)(16 / h->elem) == 0; }
 
-enum class Path { Direct, Staged, Vector, Pipe, X2, Tma, Pbb, Lean };
+enum class Path { Direct, Staged, Vector, Pipe, X2, Tma, Pbb, Lean, Pair };
 
-template <class S, class L, class LS, class LV, class LP, class LX, class LT, class LB, class LL>
+template <class S, class L, class LS, class LV, class LP, class LX, class LT, class LB, class LL,
+          class LH>
 void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged, LV launch_vec,
                LP launch_pipe, LX launch_x2, LT launch_tma, LB launch_pbb, LL launch_lean,
-               double* forces_dev) {
+               LH launch_pair, double* forces_dev) {
   wt::StepArgs<S> a = make_args<S>(h);
   const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
   const bool wide = 19 * h->n >= (1LL << 31);
@@ -194,6 +195,7 @@ void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged,
         case Path::Tma: launch_tma(a, *h->tma, h->parity, h->stream); break;
         case Path::Pbb: launch_pbb(a, grid, wide, h->stream); break;
         case Path::Lean: launch_lean(a, grid, wide, h->stream); break;
+        case Path::Pair: launch_pair(a, grid, wide, h->stream); break;
         default: launch(a, grid, wide, h->stream); break;
       }
       h->launches++;
@@ -216,10 +218,11 @@ bool x2_ok(const wt_lattice* h) {
 bool lean_ok(const wt_lattice* h);
 
 // The kernel WT_KERNEL_AUTO runs, the fastest measured on B200 for the form
-// (256x128x128 channel): the lean kernel with its L2 prefetch where it can
-// run (float32 35.1k MLUPS against 33.4k for the direct kernel, half 42.3k
-// against 37.1k), the direct kernel otherwise (exact collision, float64,
-// moving walls, buffers of 2^31 bytes or more).
+// (256x128x128 channel): the lean kernel where it can run (float32 36.7k
+// MLUPS against 33.3k for the direct kernel; half, with its L2 prefetch,
+// 44.3k against 37.2k, and 37.8k for the pair kernel), the direct kernel
+// otherwise (exact collision, float64, moving walls, buffers of 2^31 bytes
+// or more).
 Path auto_path(const wt_lattice* h) {
   if (lean_ok(h)) return Path::Lean;
   return Path::Direct;
@@ -232,6 +235,12 @@ Path auto_path(const wt_lattice* h) {
 bool lean_ok(const wt_lattice* h) {
   const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
   return !exact && !h->p.moving_walls && 19 * h->n * (long long)h->elem < (1LL << 31);
+}
+
+// True when the half-pair kernel can run: the lean kernel's conditions, half
+// storage and an even nx (32-bit pair accesses).
+bool pair_ok(const wt_lattice* h) {
+  return h->storage == WT_STORE_F16DEV && lean_ok(h) && h->nx % 2 == 0;
 }
 
 // True when the TMA tile kernel can run.
@@ -350,14 +359,16 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
   h->stats.frontal_area = 1;
   cudaGetDevice(&h->device);
   {
-    // The lean kernel prefetches the populations of the warp this many cells
-    // further on in launch order: a third of the cells its resident blocks
-    // (8 per SM) cover, the best of a sweep on B200 (0.15 to 1.2 of them).
-    // WT_PREFETCH_CELLS overrides it (0 turns the prefetch off).
+    // For half storage the lean kernel prefetches the populations of the
+    // warp this many cells further on in launch order: a third of the cells
+    // its resident blocks (8 per SM) cover, in the plateau of a sweep on B200
+    // (+7% over none from 0.15 to 0.65 of them). For float32 storage, whose
+    // loads already keep the memory system busy, any distance measured 8%
+    // slower than none, so it is off. WT_PREFETCH_CELLS overrides it (0: off).
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
     const int gx = (nx + wt::STEP_BX - 1) / wt::STEP_BX;
-    h->pf = (long long)sms * 8 * nx / gx / 3;
+    h->pf = storage == WT_STORE_F16DEV ? (long long)sms * 8 * nx / gx / 3 : 0;
     if (const char* e = getenv("WT_PREFETCH_CELLS")) h->pf = std::max(0LL, atoll(e));
   }
   h->nsegs = (long long)((nx + 31) / 32) * ny * nz;
@@ -684,6 +695,13 @@ int select_path(wt_lattice* h, Path* out) {
                     "and stationary walls");
       path = Path::Lean;
       break;
+    case WT_KERNEL_PAIR:
+      if (!pair_ok(h))
+        return fail(h, WT_ERR_UNSUPPORTED,
+                    "the pair kernel needs half storage, the float32 collision, an even nx, "
+                    "buffers under 2 GiB and stationary walls");
+      path = Path::Pair;
+      break;
     case WT_KERNEL_AUTO:
       path = auto_path(h);
       break;
@@ -702,22 +720,24 @@ void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* forces_dev) {
       if (exact) run_steps<float>(h, nsteps, path, wt::launch_step_f32_exact,
                                   wt::launch_staged_f32_exact, no_vec<float>, no_vec<float>,
                                   no_vec<float>, no_tma<float>, wt::launch_pbb_f32_exact,
-                                  wt::launch_step_f32_exact, forces_dev);
+                                  wt::launch_step_f32_exact, wt::launch_step_f32_exact,
+                                  forces_dev);
       else run_steps<float>(h, nsteps, path, wt::launch_step_f32_fast, wt::launch_staged_f32_fast,
                             wt::launch_vec_f32, wt::launch_pipe_f32, wt::launch_x2_f32,
                             wt::launch_tma_f32, wt::launch_pbb_f32_fast, wt::launch_lean_f32,
-                            forces_dev);
+                            wt::launch_lean_f32, forces_dev);
       break;
     case WT_STORE_F16DEV:
       run_steps<__half>(h, nsteps, path, wt::launch_step_f16_fast, wt::launch_staged_f16_fast,
                         wt::launch_vec_f16, wt::launch_pipe_f16, wt::launch_x2_f16,
                         wt::launch_tma_f16, wt::launch_pbb_f16_fast, wt::launch_lean_f16,
-                        forces_dev);
+                        wt::launch_pair_f16, forces_dev);
       break;
     default:
       run_steps<double>(h, nsteps, path, wt::launch_step_f64_exact, wt::launch_staged_f64_exact,
                         no_vec<double>, no_vec<double>, no_vec<double>, no_tma<double>,
-                        wt::launch_pbb_f64_exact, wt::launch_step_f64_exact, forces_dev);
+                        wt::launch_pbb_f64_exact, wt::launch_step_f64_exact,
+                        wt::launch_step_f64_exact, forces_dev);
       break;
   }
 }

@@ -121,8 +121,11 @@ struct StepArgs {
   long long nxy;       // nx*ny
   long long src[Q];    // pull offset of direction q: q*n - (ex + nx*ey + nxy*ez)
   long long dst[Q];    // store offset of direction q: q*n
-  int srcb[Q];         // src[q] and dst[q] in bytes, when both buffers span < 2^31 bytes
-  int dstb[Q];
+  // src[q] and dst[q] in bytes, when both buffers span < 2^31 bytes; both are
+  // non-negative for every lattice of at least 3 cells per axis, and unsigned
+  // so that adding one to a pointer needs no sign extension
+  uint32_t srcb[Q];
+  uint32_t dstb[Q];
   // float64 parameters (exact collision)
   double tau0, omega0, cs2, lam;
   // float32 parameters (fast collision), rounded once on the host

@@ -102,6 +102,7 @@ void launch_adj_f64(const StepArgs<double>& a, const double* Tn, double* Tc, dou
 // float32 collision, buffers under 2^31 bytes (wide is ignored).
 void launch_lean_f32(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
 void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_pair_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
 
 // Software-pipelined step launchers, float32 collision.
 void launch_pipe_f32(const StepArgs<float>& a, bool wide, cudaStream_t s);

@@ -9,6 +9,7 @@
 #include "wt_tma.cuh"
 #include "wt_pbb.cuh"
 #include "wt_lean.cuh"
+#include "wt_h2.cuh"
 
 #include <algorithm>
 
@@ -54,6 +55,11 @@ void launch_lean_f32(const StepArgs<float>& a, dim3 grid, bool, cudaStream_t s) 
 
 void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool, cudaStream_t s) {
   k_step_lean<__half><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+void launch_pair_f16(const StepArgs<__half>& a, dim3, bool, cudaStream_t s) {
+  const dim3 g((unsigned)((a.nx + 2 * H2_BX - 1) / (2 * H2_BX)), (unsigned)a.ny, (unsigned)a.nz);
+  k_step_h2<<<g, H2_BX, 0, s>>>(a);
 }
 
 // ---- partial bounce-back and adjoint (float32 arithmetic) -------------------------

@@ -302,8 +302,8 @@ struct AdjArgs {
   double wJ;       // weight of this step's force in J
   int comp;        // force component of J
   long long gat[Q];   // element offset from cell i to its link-q consumer: q*n + ex + nx ey + nxy ez
-  int gatb[Q];        // gat[q] * sizeof(T), when every offset fits in 31 bits
-  int rowb[Q];        // q*n * sizeof(T), likewise
+  uint32_t gatb[Q];   // gat[q] * sizeof(T) (non-negative), when every offset fits in 31 bits
+  uint32_t rowb[Q];   // q*n * sizeof(T), likewise
 };
 
 // The free-slip term of the adjoint of the population stored at (q, location
@@ -509,8 +509,8 @@ inline void launch_adjoint(const StepArgs<S>& a, const T* Tn, T* Tc, double* ds,
   const bool nb = 19 * a.n * (long long)wide_elem < (1LL << 31);
   for (int q = 0; q < Q; q++) {
     j.gat[q] = q * a.n + ex(q) + (long long)a.nx * ey(q) + a.nxy * ez(q);
-    j.gatb[q] = nb ? (int)(j.gat[q] * (long long)sizeof(T)) : 0;
-    j.rowb[q] = nb ? (int)(q * a.n * (long long)sizeof(T)) : 0;
+    j.gatb[q] = nb ? (uint32_t)(j.gat[q] * (long long)sizeof(T)) : 0u;
+    j.rowb[q] = nb ? (uint32_t)(q * a.n * (long long)sizeof(T)) : 0u;
   }
   const dim3 grid = step_grid(a.nx, a.ny, a.nz);
   if (nb) k_adjoint<S, T, true><<<grid, STEP_BX, 0, s>>>(a, j);
