@@ -97,8 +97,8 @@ enum {
                             stationary walls */
   WT_KERNEL_PAIR = 8     /* half storage: two cells per thread as packed half pairs (one
                             32-bit load and store per direction), each cell collided as in
-                            LEAN (bit-identical results; 18% fewer instructions, but slower
-                            than LEAN on B200); LEAN's conditions and an even nx */
+                            LEAN (bit-identical results; measured slower than LEAN on B200);
+                            LEAN's conditions and an even nx */
 };
 
 /* Rounding of half-precision stores. Stochastic rounding draws its random

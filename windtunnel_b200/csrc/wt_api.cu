@@ -220,7 +220,7 @@ bool lean_ok(const wt_lattice* h);
 // The kernel WT_KERNEL_AUTO runs, the fastest measured on B200 for the form
 // (256x128x128 channel): the lean kernel where it can run (float32 36.7k
 // MLUPS against 33.3k for the direct kernel; half, with its L2 prefetch,
-// 44.3k against 37.2k, and 37.8k for the pair kernel), the direct kernel
+// 44.3k against 37.2k, and 39.7k for the pair kernel), the direct kernel
 // otherwise (exact collision, float64, moving walls, buffers of 2^31 bytes
 // or more).
 Path auto_path(const wt_lattice* h) {

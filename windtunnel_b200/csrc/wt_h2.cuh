@@ -12,8 +12,11 @@
 // Cell A is unpacked to floats, collided and rounded back into the low
 // halves; then cell B from the high halves, by the same code (a loop over
 // the two cells that is not unrolled, so the collision is one copy in the
-// instruction cache); the live state stays at 19 packed words plus one
-// cell's 19 floats.
+// instruction cache). The launched form parks the packed words in the
+// thread's column of shared memory meanwhile (64 registers); the register
+// form needs 96. On B200 both ran slower than the lean kernel (39.7k and
+// 37.8k against 44.3k MLUPS on 256x128x128): the kernel is kept as a
+// selectable alternative (WT_KERNEL_PAIR).
 //
 // Requirements (checked by the host): half storage, the float32 collision,
 // stationary walls, nx even, buffers under 2^31 bytes.
@@ -57,17 +60,38 @@ __device__ __forceinline__ uint32_t set_half(uint32_t w, int sh, __half h) {
   return (w & ~(0xffffu << sh)) | ((uint32_t)__half_as_ushort(h) << sh);
 }
 
+// Where a thread keeps its 19 packed words between the pulls and the stores:
+// in registers (RegWords), or in its column of a shared-memory array
+// (SmemWords), which frees 19 registers for the collision so that the
+// kernel fits the 64 registers of 32 resident warps per SM.
+struct RegWords {
+  uint32_t w[Q];
+  __device__ __forceinline__ uint32_t get(int q) const { return w[q]; }
+  __device__ __forceinline__ void put(int q, uint32_t v) { w[q] = v; }
+  __device__ __forceinline__ void put_half(int q, int sh, __half h) { w[q] = set_half(w[q], sh, h); }
+};
+struct SmemWords {
+  uint32_t (*s)[H2_BX];   // [Q][H2_BX]: consecutive threads, consecutive words
+  int t;
+  __device__ __forceinline__ uint32_t get(int q) const { return s[q][t]; }
+  __device__ __forceinline__ void put(int q, uint32_t v) { s[q][t] = v; }
+  __device__ __forceinline__ void put_half(int q, int sh, __half h) {
+    reinterpret_cast<__half*>(&s[q][t])[sh >> 4] = h;
+  }
+};
+
 // Collide the cell at bit offset sh of the pair in place: the pulled values
 // are unpacked, patched, collided and rounded back into the same halves;
 // r, v the cell's density (storage units) and velocity. One copy of this
 // code serves both cells (the caller loops over them without unrolling).
-__device__ __forceinline__ void collide_half(const StepArgs<__half>& a, uint32_t (&w)[Q], int sh,
+template <class W>
+__device__ __forceinline__ void collide_half(const StepArgs<__half>& a, W& w, int sh,
                                              long long i, int x, int y, int z, bool wall,
                                              bool shell, double& Fx, double& Fy, double& Fz,
                                              float& r, float& vx, float& vy, float& vz) {
   float f[Q];
 #pragma unroll
-  for (int q = 0; q < Q; q++) f[q] = half_at(w[q], sh);
+  for (int q = 0; q < Q; q++) f[q] = half_at(w.get(q), sh);
   if (wall || shell) patch_raw<__half, 0>(a, i, x, y, z, wall, shell, f, Fx, Fy, Fz);
   collide_x2<__half, float>(a, f, r, vx, vy, vz);
   if (a.f16_sr) {
@@ -78,18 +102,22 @@ __device__ __forceinline__ void collide_half(const StepArgs<__half>& a, uint32_t
     for (int k = 1; k < Q; k += 2) {
       h ^= h << 13; h ^= h >> 17; h ^= h << 5;
       const __half2 p = sr_half2(f[k], f[k + 1], h);
-      w[k] = set_half(w[k], sh, __high2half(p));
-      w[k + 1] = set_half(w[k + 1], sh, __low2half(p));
+      w.put_half(k, sh, __high2half(p));
+      w.put_half(k + 1, sh, __low2half(p));
     }
     h ^= h << 13; h ^= h >> 17; h ^= h << 5;
-    w[0] = set_half(w[0], sh, __low2half(sr_half2(0.0f, f[0], h)));
+    w.put_half(0, sh, __low2half(sr_half2(0.0f, f[0], h)));
   } else {
 #pragma unroll
-    for (int q = 0; q < Q; q++) w[q] = set_half(w[q], sh, __float2half_rn(f[q]));
+    for (int q = 0; q < Q; q++) w.put_half(q, sh, __float2half_rn(f[q]));
   }
 }
 
-__global__ void __launch_bounds__(H2_BX, 10) k_step_h2(const __grid_constant__ StepArgs<__half> a) {
+// SMEM: the packed words live in shared memory between the pulls and the
+// stores (64 registers, 16 blocks per SM) instead of registers (96, 10).
+template <bool SMEM>
+__global__ void __launch_bounds__(H2_BX, SMEM ? 16 : 10)
+    k_step_h2(const __grid_constant__ StepArgs<__half> a) {
   constexpr float SC = X2<__half>::SC;
   const int t = threadIdx.x;
   const int lane = t & 31;
@@ -127,17 +155,22 @@ __global__ void __launch_bounds__(H2_BX, 10) k_step_h2(const __grid_constant__ S
 
   // the pulled pairs of an interior row (every lane takes part in the
   // shuffles); the floor row pulls nothing
-  uint32_t w[Q];
+  __shared__ uint32_t sw[SMEM ? Q : 1][H2_BX];
+  typename std::conditional<SMEM, SmemWords, RegWords>::type w;
+  if constexpr (SMEM) {
+    w.s = sw;
+    w.t = t;
+  }
   if (y >= 1) {
     const char* Fb = reinterpret_cast<const char*>(a.F + i0);
-#define WT_PULL(q) w[q] = pull_word<q>(Fb, a.srcb[q], lane, active);
+#define WT_PULL(q) w.put(q, pull_word<q>(Fb, a.srcb[q], lane, active));
     WT_PULL(0) WT_PULL(1) WT_PULL(2) WT_PULL(3) WT_PULL(4) WT_PULL(5) WT_PULL(6) WT_PULL(7)
     WT_PULL(8) WT_PULL(9) WT_PULL(10) WT_PULL(11) WT_PULL(12) WT_PULL(13) WT_PULL(14)
     WT_PULL(15) WT_PULL(16) WT_PULL(17) WT_PULL(18)
 #undef WT_PULL
   } else {
 #pragma unroll
-    for (int q = 0; q < Q; q++) w[q] = 0u;
+    for (int q = 0; q < Q; q++) w.put(q, 0u);
   }
   if (active) {
     const uint16_t fl2 = *reinterpret_cast<const uint16_t*>(a.flags + i0);
@@ -163,7 +196,7 @@ __global__ void __launch_bounds__(H2_BX, 10) k_step_h2(const __grid_constant__ S
         }
       } else if (cat == CAT_EQ) {
 #pragma unroll
-        for (int q = 0; q < Q; q++) w[q] = set_half(w[q], sh, a.eq[q]);
+        for (int q = 0; q < Q; q++) w.put_half(q, sh, a.eq[q]);
         if (a.write_fields) { a.ux[i] = a.u0f; a.uy[i] = 0.0f; a.uz[i] = 0.0f; a.rho[i] = 1.0f; }
       }
     }
@@ -173,10 +206,13 @@ __global__ void __launch_bounds__(H2_BX, 10) k_step_h2(const __grid_constant__ S
       // step (a solid cell there keeps its stale populations and fields)
       if (catA == CAT_KEEP) {
 #pragma unroll
-        for (int q = 0; q < Q; q++) w[q] = set_half(w[q], 16, gh(q, 0));
+        for (int q = 0; q < Q; q++) w.put_half(q, 16, gh(q, 0));
       } else {
 #pragma unroll
-        for (int q = 0; q < Q; q++) w[q] = (w[q] & 0xffffu) | (w[q] << 16);
+        for (int q = 0; q < Q; q++) {
+          const uint32_t v = w.get(q);
+          w.put(q, (v & 0xffffu) | (v << 16));
+        }
       }
       if (a.write_fields) {
         a.ux[iB] = a.ux[i0]; a.uy[iB] = a.uy[i0]; a.uz[iB] = a.uz[i0]; a.rho[iB] = a.rho[i0];
@@ -185,13 +221,13 @@ __global__ void __launch_bounds__(H2_BX, 10) k_step_h2(const __grid_constant__ S
     const bool storeA = catA != CAT_KEEP, storeB = catB != CAT_KEEP;
     if (storeA && storeB) {
 #pragma unroll
-      for (int q = 0; q < Q; q++) gw(q) = w[q];
+      for (int q = 0; q < Q; q++) gw(q) = w.get(q);
     } else if (storeA) {
 #pragma unroll
-      for (int q = 0; q < Q; q++) gh(q, 0) = __ushort_as_half((unsigned short)(w[q] & 0xffffu));
+      for (int q = 0; q < Q; q++) gh(q, 0) = __ushort_as_half((unsigned short)(w.get(q) & 0xffffu));
     } else if (storeB) {
 #pragma unroll
-      for (int q = 0; q < Q; q++) gh(q, 1) = __ushort_as_half((unsigned short)(w[q] >> 16));
+      for (int q = 0; q < Q; q++) gh(q, 1) = __ushort_as_half((unsigned short)(w.get(q) >> 16));
     }
   }
   constexpr double inv_sc = 1.0 / (double)SC;   // a power of two: exact

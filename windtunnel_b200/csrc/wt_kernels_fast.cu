@@ -59,7 +59,7 @@ void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool, cudaStream_t s)
 
 void launch_pair_f16(const StepArgs<__half>& a, dim3, bool, cudaStream_t s) {
   const dim3 g((unsigned)((a.nx + 2 * H2_BX - 1) / (2 * H2_BX)), (unsigned)a.ny, (unsigned)a.nz);
-  k_step_h2<<<g, H2_BX, 0, s>>>(a);
+  k_step_h2<true><<<g, H2_BX, 0, s>>>(a);
 }
 
 // ---- partial bounce-back and adjoint (float32 arithmetic) -------------------------
