@@ -249,14 +249,19 @@ typedef struct wt_adj_cfg {
   int32_t checkpoint;  /* steps between stored states; 0 = every state when
                           (nsteps + 3) states fit in 3/4 of the free device
                           memory, else ceil(sqrt(nsteps)) */
-  int32_t reserved[4]; /* must be 0 */
+  int32_t keep;        /* nonzero: leave this run's device memory (checkpoints, interval
+                          store, adjoint buffers) in the lattice for the next wt_adjoint
+                          call that fits in it, as an optimisation loop wants; 0: free it,
+                          and any memory an earlier call kept, when the call ends.
+                          wt_destroy frees kept memory. */
+  int32_t reserved[3]; /* must be 0 */
 } wt_adj_cfg;
 
 typedef struct wt_adj_stats {
   double J;            /* the objective */
   double forward_ms;   /* forward sweep with checkpoint copies (CUDA events) */
   double backward_ms;  /* recomputation + adjoint steps (CUDA events) */
-  int64_t device_bytes;/* device memory the run allocated (checkpoints, segment, adjoint) */
+  int64_t device_bytes;/* device memory the run used (checkpoints, segment, adjoint) */
   int32_t checkpoints; /* checkpoint intervals */
   int32_t segment;     /* steps per checkpoint interval */
 } wt_adj_stats;

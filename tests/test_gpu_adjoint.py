@@ -92,6 +92,25 @@ def test_adjoint_leaves_the_stepped_state(wt_lib, checkpoint):
         assert np.array_equal(x, y)
 
 
+def test_adjoint_keep_reuses_memory(wt_lib):
+    """keep leaves the run's device memory in the lattice: a second and a
+    smaller run reuse it and give bit-identical gradients; a larger run
+    replaces it; a run without keep frees it."""
+    import torch
+    N, W = 40, 15
+    _, g_ref, st_ref = _gpu("f32").adjoint(N, W, checkpoint=6)
+    sim = _gpu("f32")
+    start = sim.get_state()
+    free0 = torch.cuda.mem_get_info()[0]
+    for c, keep in ((6, True), (6, True), (10, True), (3, True), (6, False)):
+        sim.set_state(start)
+        _, g, st = sim.adjoint(N, W, checkpoint=c, keep=keep)
+        if c == 6:
+            assert np.array_equal(g, g_ref)
+            assert st["device_bytes"] == st_ref["device_bytes"]
+    assert torch.cuda.mem_get_info()[0] >= free0 - (8 << 20)
+
+
 def test_adjoint_f32_close_to_f64(wt_lib, oracle_lib):
     N, W = 40, 15
     _, gf, _ = _gpu("f32", math="fast").adjoint(N, W)

@@ -94,7 +94,7 @@ class wt_body_stats(C.Structure):
 
 class wt_adj_cfg(C.Structure):
     _fields_ = [("nsteps", C.c_int32), ("window", C.c_int32), ("component", C.c_int32),
-                ("checkpoint", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("checkpoint", C.c_int32), ("keep", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class wt_adj_stats(C.Structure):

@@ -18,14 +18,14 @@ from .lbm import LBM
 class DragFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, s: torch.Tensor, sim: LBM, box, nsteps: int, window: int,
-                component: int = 0, checkpoint: int = 0):
+                component: int = 0, checkpoint: int = 0, keep: bool = False):
         sv = s.detach().to("cpu", torch.float64).numpy()
         sim.set_solid_fraction(box, sv)
         start = sim.get_state()
         f = sim.step_forces(int(nsteps))
         J = float(f[-int(window):, component].mean())
         ctx.sim, ctx.box, ctx.start, ctx.sv = sim, box, start, sv
-        ctx.cfg = (int(nsteps), int(window), int(component), int(checkpoint))
+        ctx.cfg = (int(nsteps), int(window), int(component), int(checkpoint), bool(keep))
         ctx.s_meta = (s.dtype, s.device)
         return torch.tensor(J, dtype=torch.float64)
 
@@ -39,10 +39,12 @@ class DragFn(torch.autograd.Function):
         sim.set_state(end)   # the lattice stays where the forward pass left it
         dtype, device = ctx.s_meta
         grad = torch.from_numpy(np.ascontiguousarray(g)).to(device=device, dtype=dtype)
-        return gJ.to(dtype) * grad, None, None, None, None, None, None
+        return gJ.to(dtype) * grad, None, None, None, None, None, None, None
 
 
 def drag(s: torch.Tensor, sim: LBM, box, nsteps: int, window: int, component: int = 0,
-         checkpoint: int = 0) -> torch.Tensor:
-    """Time-averaged force component with the discrete adjoint as its gradient."""
-    return DragFn.apply(s, sim, box, nsteps, window, component, checkpoint)
+         checkpoint: int = 0, keep: bool = False) -> torch.Tensor:
+    """Time-averaged force component with the discrete adjoint as its gradient.
+    keep: the backward pass leaves its device memory in `sim` for the next
+    backward (an optimisation loop over the same lattice)."""
+    return DragFn.apply(s, sim, box, nsteps, window, component, checkpoint, keep)

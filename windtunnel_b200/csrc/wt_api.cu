@@ -78,6 +78,8 @@ void free_all(wt_lattice* h) {
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h->tma;
   h->tma = nullptr;
+  if (h->adj_pool) cudaFree(h->adj_pool);
+  h->adj_pool = nullptr;
 }
 
 int check_params(const wt_params* p) {
@@ -1026,18 +1028,46 @@ extern "C" int wt_set_solid_fraction(wt_lattice* h, const int box[6], const doub
 namespace {
 
 // Device buffers of one adjoint run, released on every exit path.
-struct AdjBuffers {
-  std::vector<void*> ptrs;
-  size_t bytes = 0;
-  void* get(size_t n) {
+// The adjoint's device memory (checkpoints, interval store, two adjoint
+// buffers, dJ/ds, the force series) as one block carved in order. A run with
+// cfg.keep leaves the block in the lattice for the next run that fits in it
+// (an optimisation loop then pays for cudaMalloc / cudaFree once); a run
+// without it frees any kept block when it ends, on every return path.
+struct AdjBlock {
+  wt_lattice* h;
+  bool keep;
+  size_t off = 0;
+  unsigned char* base = nullptr;
+  static size_t up(size_t n) { return (n + 255) & ~(size_t)255; }
+  // one block of `total` bytes: the kept one if it is large enough
+  bool acquire(size_t total) {
+    if (h->adj_pool && h->adj_pool_bytes >= total) {
+      base = (unsigned char*)h->adj_pool;
+      return true;
+    }
+    release();
     void* p = nullptr;
-    if (cudaMalloc(&p, n) != cudaSuccess) return nullptr;
-    ptrs.push_back(p);
-    bytes += n;
+    if (cudaMalloc(&p, total) != cudaSuccess) return false;
+    h->adj_pool = p;
+    h->adj_pool_bytes = total;
+    base = (unsigned char*)p;
+    return true;
+  }
+  void* carve(size_t n) {
+    void* p = base + off;
+    off += up(n);
     return p;
   }
-  ~AdjBuffers() {
-    for (void* p : ptrs) cudaFree(p);
+  void release() {
+    if (h->adj_pool) {
+      cudaStreamSynchronize(h->stream);
+      cudaFree(h->adj_pool);
+    }
+    h->adj_pool = nullptr;
+    h->adj_pool_bytes = 0;
+  }
+  ~AdjBlock() {
+    if (!keep) release();
   }
 };
 
@@ -1050,19 +1080,22 @@ int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_ad
   const int ncp = (N + C - 1) / C;
   const int* b = h->sbox;
   const size_t nbox = (size_t)(b[3] - b[0]) * (b[4] - b[1]) * (b[5] - b[2]);
-  AdjBuffers mem;
+  AdjBlock mem{h, cfg.keep != 0};
   const size_t pel = pop / sizeof(S);                // elements of one state
   // checkpoints S^{kC} of every segment but the last, whose states the
   // forward sweep writes straight into the segment store (C + 1 states)
-  S* cps = ncp > 1 ? (S*)mem.get(pop * (size_t)(ncp - 1)) : nullptr;
-  S* seg = (S*)mem.get(pop * (size_t)(C + 1));
-  T* Tbuf[2] = {(T*)mem.get(tsz), (T*)mem.get(tsz)};
-  double* ds = (double*)mem.get(sizeof(double) * nbox);
-  double* fdev = (double*)mem.get(sizeof(double) * 3 * (size_t)N);
-  if ((ncp > 1 && !cps) || !seg || !Tbuf[0] || !Tbuf[1] || !ds || !fdev)
+  const size_t sz_cps = ncp > 1 ? pop * (size_t)(ncp - 1) : 0, sz_seg = pop * (size_t)(C + 1);
+  const size_t sz_ds = sizeof(double) * nbox, sz_f = sizeof(double) * 3 * (size_t)N;
+  const size_t total = AdjBlock::up(sz_cps) + AdjBlock::up(sz_seg) + 2 * AdjBlock::up(tsz) +
+                       AdjBlock::up(sz_ds) + AdjBlock::up(sz_f);
+  if (!mem.acquire(total))
     return fail(h, WT_ERR_OOM, "cannot allocate the adjoint's checkpoints (" +
-                                   std::to_string((pop * (size_t)(ncp + C) + 2 * tsz) >> 20) +
-                                   " MiB)");
+                                   std::to_string(total >> 20) + " MiB)");
+  S* cps = ncp > 1 ? (S*)mem.carve(sz_cps) : nullptr;
+  S* seg = (S*)mem.carve(sz_seg);
+  T* Tbuf[2] = {(T*)mem.carve(tsz), (T*)mem.carve(tsz)};
+  double* ds = (double*)mem.carve(sz_ds);
+  double* fdev = (double*)mem.carve(sz_f);
   cudaEvent_t e0, e1, e2;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -1156,7 +1189,7 @@ int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_ad
     st->J = J;
     st->forward_ms = fwd_ms;
     st->backward_ms = bwd_ms;
-    st->device_bytes = (int64_t)mem.bytes;
+    st->device_bytes = (int64_t)total;
     st->checkpoints = ncp;
     st->segment = C;
   }
@@ -1170,9 +1203,10 @@ extern "C" int wt_adjoint(wt_lattice* h, const wt_adj_cfg* cfg, double* dJds, wt
   if (!cfg || !dJds) return fail(h, WT_ERR_ARG, "cfg and dJds are required");
   if (!h->sfrac) return fail(h, WT_ERR_STATE, "set a solid-fraction field first");
   if (cfg->nsteps < 1 || cfg->window < 1 || cfg->window > cfg->nsteps || cfg->component < 0 ||
-      cfg->component > 2 || cfg->checkpoint < 0)
+      cfg->component > 2 || cfg->checkpoint < 0 || cfg->reserved[0] || cfg->reserved[1] ||
+      cfg->reserved[2])
     return fail(h, WT_ERR_ARG, "need nsteps >= 1, 1 <= window <= nsteps, component 0..2, "
-                               "checkpoint >= 0");
+                               "checkpoint >= 0, reserved fields 0");
   if (h->p.moving_walls)
     return fail(h, WT_ERR_UNSUPPORTED, "the adjoint supports stationary walls only");
   if (h->p.kernel != WT_KERNEL_AUTO && h->p.kernel != WT_KERNEL_DIRECT)

@@ -43,6 +43,8 @@ struct wt_lattice {
   long long* diag_dev = nullptr; // first rejected staged copy {kind, q, unit, offset}
   wt::TmaMaps* tma = nullptr;    // tensor maps of the TMA tile kernel (host copy), or null
   double* sfrac = nullptr;       // partial bounce-back solid fraction on sbox (device), or null
+  void* adj_pool = nullptr;      // device memory a wt_adjoint run with keep left for the next
+  size_t adj_pool_bytes = 0;
   int sbox[6] = {0, 0, 0, 0, 0, 0};
   // voxelize statistics scratch
   uint8_t* col = nullptr;        // ny*nz frontal projection

@@ -423,12 +423,16 @@ class LBM:
         self._call(lib().wt_set_solid_fraction, b, _dptr(a))
         self._sbox = tuple(int(v) for v in box)
 
-    def adjoint(self, nsteps: int, window: int, component: int = 0, checkpoint: int = 0):
+    def adjoint(self, nsteps: int, window: int, component: int = 0, checkpoint: int = 0,
+                keep: bool = False):
         """(J, dJ/ds as [z][y][x] over the box, stats): J is the mean force component
-        over the last `window` of `nsteps` steps from the current state."""
+        over the last `window` of `nsteps` steps from the current state. keep leaves
+        the run's device memory in the lattice for the next call (an optimisation
+        loop); a call without it frees that memory."""
         x0, y0, z0, x1, y1, z1 = self._sbox
         g = np.empty((z1 - z0, y1 - y0, x1 - x0), np.float64)
-        cfg = W.wt_adj_cfg(int(nsteps), int(window), int(component), int(checkpoint))
+        cfg = W.wt_adj_cfg(int(nsteps), int(window), int(component), int(checkpoint),
+                           int(bool(keep)))
         st = W.wt_adj_stats()
         self._call(lib().wt_adjoint, C.byref(cfg), _dptr(g), C.byref(st))
         self._fields_at = -1
