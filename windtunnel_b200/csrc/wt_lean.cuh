@@ -27,8 +27,16 @@ __device__ __forceinline__ long long lean_off(uint32_t b) {
   else return (long long)b;
 }
 
+// Resident blocks per SM the register budget is set for: float32 storage
+// fits 72 registers without spills at 7 (28 warps; +3% over 64 registers
+// and 8 blocks on B200), half storage is issue-bound and runs best at 8
+// (32 warps, 64 registers; 7 measured -4%).
 template <class S>
-__global__ void __launch_bounds__(STEP_BX, 8) k_step_lean(const __grid_constant__ StepArgs<S> a) {
+constexpr int lean_min_blocks() { return sizeof(S) == 4 ? 7 : 8; }
+
+template <class S>
+__global__ void __launch_bounds__(STEP_BX, lean_min_blocks<S>())
+    k_step_lean(const __grid_constant__ StepArgs<S> a) {
   using T = X2<S>;
   constexpr float SC = T::SC;
   const int x = blockIdx.x * STEP_BX + threadIdx.x;
