@@ -75,19 +75,27 @@ WORKLOADS = {
 _GRIDS = {}
 
 
-def body_inputs(wl):
+def body_inputs(wl, on_gpu: bool = True):
     """The benchmark body: a seeded 20000-triangle superellipsoid hull with a
     radial bump field, oriented and length-normalised (Shapes.orient), voxelised
-    on the GPU with Voxel.build at `res` cells along its length, placed at
-    scale / yaw / pos by the device lookup."""
+    with Voxel.build at `res` cells along its length (on the GPU, or for the
+    CPU arms by the oracle's restatement, which gives the same grid bit for
+    bit), placed at scale / yaw / pos by the lookup."""
     from windtunnel_b200.bodies import body_box, body_matrix
-    from windtunnel_b200.mesh import hull_mesh, orient, voxel_build
+    from windtunnel_b200.mesh import VoxelGrid, hull_mesh, orient, voxel_build
     b = wl["body"]
-    key = (b["semi"], b["exponent"], b["res"])
+    key = (b["semi"], b["exponent"], b["res"], on_gpu)
     if key not in _GRIDS:
         tris = hull_mesh(semi=b["semi"], exponent=b["exponent"], seed=wl["seed"])
         orient(tris, 0, 1)
-        _GRIDS[key] = voxel_build(tris, b["res"])
+        if on_gpu:
+            _GRIDS[key] = voxel_build(tris, b["res"])
+        else:
+            from oracle.oracle import voxel_build as oracle_voxel_build
+            grid, info = oracle_voxel_build(tris, b["res"])
+            _GRIDS[key] = VoxelGrid(grid=grid, **{k: info[k] for k in (
+                "nx", "ny", "nz", "cell", "min", "inv", "ext", "centre", "bbox", "tris",
+                "solid", "openness")})
     vg = _GRIDS[key]
     M = body_matrix(math.radians(b["yaw_deg"]), 0.0)
     P = [0.36 * wl["nx"], 0.5 * wl["ny"], 0.5 * wl["nz"]]
@@ -115,7 +123,7 @@ def setup_oracle(wl):
     o = OracleLBM(wl["nx"], wl["ny"], wl["nz"], "f32", side_bc=wl["side_bc"])
     o.set_params(u0=wl["u0"], tau=wl["tau"], csm=wl["csm"], les=int(wl["les"]),
                  **{"lambda": wl["lam"]})
-    vg, M, P, box = body_inputs(wl)
+    vg, M, P, box = body_inputs(wl, on_gpu=False)
     mask = lookup_mask(vg.grid, vg.min, vg.inv, M, P, wl["body"]["scale"], wl["nx"], wl["ny"],
                        wl["nz"], box)
     o.voxelize_mask(box, mask)
