@@ -90,11 +90,11 @@ enum {
                             nearest rounding for half storage */
   WT_KERNEL_LEAN = 7,    /* one thread per cell, 32-bit byte offsets from one pointer per cell,
                             the collision in storage units with approximate reciprocal / square
-                            root, and for half storage an L2 prefetch of the populations a
-                            fixed distance ahead in launch order (environment
-                            WT_PREFETCH_CELLS overrides the distance at wt_create, for either
-                            storage; 0 turns it off); float32 collision, buffers under 2 GiB,
-                            stationary walls */
+                            root, and for half storage on lattices whose population buffer
+                            fits in twice the L2 an L2 prefetch of the populations a fixed
+                            distance ahead in launch order (environment WT_PREFETCH_CELLS
+                            overrides the distance at wt_create, for any lattice; 0 turns it
+                            off); float32 collision, buffers under 2 GiB, stationary walls */
   WT_KERNEL_PAIR = 8     /* half storage: two cells per thread as packed half pairs (one
                             32-bit load and store per direction), each cell collided as in
                             LEAN (bit-identical results; measured slower than LEAN on B200);

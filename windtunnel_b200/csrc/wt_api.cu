@@ -361,16 +361,20 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
   h->stats.frontal_area = 1;
   cudaGetDevice(&h->device);
   {
-    // For half storage the lean kernel prefetches the populations of the
-    // warp this many cells further on in launch order: a third of the cells
-    // its resident blocks (8 per SM) cover, in the plateau of a sweep on B200
-    // (+7% over none from 0.15 to 0.65 of them). For float32 storage, whose
-    // loads already keep the memory system busy, any distance measured 8%
-    // slower than none, so it is off. WT_PREFETCH_CELLS overrides it (0: off).
-    int sms = 0;
+    // The lean kernel can prefetch into L2 the populations of the warp this
+    // many cells further on in launch order: a third of the cells its
+    // resident blocks (8 per SM) cover. Measured on B200 it pays only for half
+    // storage on lattices whose population buffer fits in twice the L2
+    // (256x128x128: +7% over none, flat from 0.15 to 0.65 of the resident
+    // cells); it cost 8% for float32 storage on the same lattice and 19% for
+    // half storage on 512x192x192, whatever the distance, so it is off there.
+    // WT_PREFETCH_CELLS overrides it (0: off).
+    int sms = 0, l2 = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, h->device);
     const int gx = (nx + wt::STEP_BX - 1) / wt::STEP_BX;
-    h->pf = storage == WT_STORE_F16DEV ? (long long)sms * 8 * nx / gx / 3 : 0;
+    const bool small = (double)n * 19 * elem_size(storage) <= 2.0 * (double)l2;
+    h->pf = storage == WT_STORE_F16DEV && small ? (long long)sms * 8 * nx / gx / 3 : 0;
     if (const char* e = getenv("WT_PREFETCH_CELLS")) h->pf = std::max(0LL, atoll(e));
   }
   h->nsegs = (long long)((nx + 31) / 32) * ny * nz;
