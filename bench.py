@@ -234,21 +234,27 @@ def profiled_traffic(kernel_tag: str) -> float | None:
 
 
 class Dist:
-    def __init__(self):
+    """One rank per GPU from the torchrun environment: barriers and the max of
+    a time over ranks. backend "nccl" (the GPU runs) or "gloo" (CPU ranks,
+    which the tests use)."""
+
+    def __init__(self, backend: str = "nccl"):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = False
 
     def init(self):
-        import torch
-        torch.cuda.set_device(self.local)
-        if self.world > 1:
-            import datetime
+        import datetime
 
+        import torch
+        if self.backend == "nccl":
+            torch.cuda.set_device(self.local)
+        if self.world > 1:
             import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
-                                    device_id=torch.device("cuda", self.local))
+            kw = {"device_id": torch.device("cuda", self.local)} if self.backend == "nccl" else {}
+            dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=180), **kw)
             self.pg = True
 
     def barrier(self):
@@ -261,7 +267,8 @@ class Dist:
             return v
         import torch
         import torch.distributed as dist
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -269,6 +276,12 @@ class Dist:
         if self.pg:
             import torch.distributed as dist
             dist.destroy_process_group()
+
+
+def whole_job_mlups(world: int, cells: int, steps: int, ms_max: float) -> float:
+    """Replicas: every rank steps its own lattice of `cells` cells, so the job
+    updates world x cells x steps cells in the slowest rank's time."""
+    return world * cells * steps / (ms_max * 1e-3) / 1e6
 
 
 def timed_steps(sim, K: int, dist: Dist) -> tuple[float, int]:
@@ -581,7 +594,7 @@ def run_wt(args) -> None:
     ms, launches = timed_steps(sim, K, dist)
     clk = clocks.stop() if clocks else None
     ms_max = dist.max(ms)
-    value = dist.world * n * K / (ms_max * 1e-3) / 1e6
+    value = whole_job_mlups(dist.world, n, K, ms_max)
 
     # public per-step path (host buffers, one sync per step)
     sim.step_forces(W)
@@ -591,8 +604,8 @@ def run_wt(args) -> None:
     from windtunnel_b200._lib import wt_params
     import ctypes
     h2d = ctypes.sizeof(wt_params)
-    e2e_val = dist.world * n * ke / (e2e_ms * 1e-3) / 1e6
-    e2e1_val = dist.world * n * ke / (e2e1_ms * 1e-3) / 1e6
+    e2e_val = whole_job_mlups(dist.world, n, ke, e2e_ms)
+    e2e1_val = whole_job_mlups(dist.world, n, ke, e2e1_ms)
     sim.close()
 
     # half-deviation storage on the same workload
@@ -600,7 +613,7 @@ def run_wt(args) -> None:
     s16.step_forces(W)
     ms16, _ = timed_steps(s16, K, dist)
     ms16 = dist.max(ms16)
-    v16 = dist.world * n * K / (ms16 * 1e-3) / 1e6
+    v16 = whole_job_mlups(dist.world, n, K, ms16)
     s16.close()
     # ... and with stochastic rounding of the half stores
     s16 = setup_gpu(wl, "f16dev", "fast")
@@ -608,7 +621,7 @@ def run_wt(args) -> None:
     s16.step_forces(W)
     ms16s, _ = timed_steps(s16, K, dist)
     ms16s = dist.max(ms16s)
-    v16s = dist.world * n * K / (ms16s * 1e-3) / 1e6
+    v16s = whole_job_mlups(dist.world, n, K, ms16s)
     s16.close()
 
     achieved = BYTES_PER_CELL["f32"] * n * K / (ms * 1e-3) / 1e9
