@@ -342,13 +342,15 @@ __device__ __forceinline__ T adj_shell(const StepArgs<S>& a, const T* Tn, int q,
 // values it pulled; cells of the solid-fraction box also accumulate dJ/ds.
 // NB: offsets in bytes (every buffer spans < 2^31 bytes) instead of 64-bit
 // element indices.
-// Resident blocks per SM the register budget is set for: float32 adjoints
-// fit 96 registers without spilling (20 warps per SM); float64 ones take 168.
-template <class T>
-constexpr int adj_min_blocks() { return sizeof(T) == 4 ? 5 : 3; }
+// Resident blocks per SM the register budget is set for, the fastest measured
+// on B200: float32 adjoints of a half-storage state 5 (96 registers; 4
+// measured 7% slower), of a float32 state 4 (128 registers, no spills; 3%
+// faster than 5); float64 adjoints 3 (168 registers).
+template <class S, class T>
+constexpr int adj_min_blocks() { return sizeof(T) == 8 ? 3 : (sizeof(S) == 4 ? 4 : 5); }
 
 template <class S, class T, bool NB>
-__global__ void __launch_bounds__(STEP_BX, adj_min_blocks<T>()) k_adjoint(const __grid_constant__ StepArgs<S> a,
+__global__ void __launch_bounds__(STEP_BX, adj_min_blocks<S, T>()) k_adjoint(const __grid_constant__ StepArgs<S> a,
                                                          const __grid_constant__ AdjArgs<T> j) {
   const int x = blockIdx.x * STEP_BX + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
