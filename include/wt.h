@@ -95,10 +95,15 @@ enum {
                             distance ahead in launch order (environment WT_PREFETCH_CELLS
                             overrides the distance at wt_create, for any lattice; 0 turns it
                             off); float32 collision, buffers under 2 GiB, stationary walls */
-  WT_KERNEL_PAIR = 8     /* half storage: two cells per thread as packed half pairs (one
+  WT_KERNEL_PAIR = 8,    /* half storage: two cells per thread as packed half pairs (one
                             32-bit load and store per direction), each cell collided as in
                             LEAN (bit-identical results; measured slower than LEAN on B200);
                             LEAN's conditions and an even nx */
+  WT_KERNEL_TILE = 9     /* a block's 128 cells of a row: its 19 source row segments copied
+                            into shared memory with 16-byte loads, each cell collided as in
+                            LEAN from there (bit-identical results), the outputs written back
+                            with 16-byte stores (measured slower than LEAN on B200); LEAN's
+                            conditions and nx a multiple of 8 */
 };
 
 /* Rounding of half-precision stores. Stochastic rounding draws its random

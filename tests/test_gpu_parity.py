@@ -335,6 +335,50 @@ def test_pair_kernel_bit_identical_to_lean(both, dims, rounding, side_bc):
     assert np.array_equal(ga, gb)
 
 
+@pytest.mark.parametrize("dims", [(40, 14, 12), (64, 20, 18), (128, 9, 9), (264, 10, 9)])
+@pytest.mark.parametrize("storage,rounding", [("f32", "nearest"), ("f16dev", "nearest"),
+                                              ("f16dev", "stochastic")])
+@pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
+def test_tile_kernel_bit_identical_to_lean(both, dims, storage, rounding, side_bc):
+    """The shared-memory tile kernel pulls the same values and collides each
+    cell as the lean kernel does: populations (both buffers), fields and the
+    force series are bit-identical, with a body touching the outlet column,
+    a road, either side condition, and rows of one block, one full block and
+    two blocks and a partial one."""
+    LBM, _ = both
+    out = []
+    for kern in ("lean", "tile"):
+        s = LBM(*dims, storage=storage, kernel=kern, side_bc=side_bc)
+        if storage == "f16dev":
+            s.set_params(f16_rounding=rounding)
+        apply_case(s, sphere=(dims[0] - 4.5, dims[1] / 2, dims[2] / 2, 3.3), side_bc=side_bc,
+                   ground=True)
+        f1 = s.step_forces(7)
+        u1 = s.fields()
+        f2 = s.step_forces(18)
+        out.append((np.concatenate([f1, f2]), u1, s.fields(), s.populations("f", "raw"),
+                    s.populations("g", "raw")))
+    (fa, ua1, ua2, pa, ga), (fb, ub1, ub2, pb, gb) = out
+    assert np.array_equal(fa, fb)
+    for a, b in list(zip(ua1, ub1)) + list(zip(ua2, ub2)):
+        assert np.array_equal(a, b)
+    assert np.array_equal(pa, pb)
+    assert np.array_equal(ga, gb)
+
+
+def test_tile_kernel_conditions(both):
+    from windtunnel_b200 import WTError
+    LBM, _ = both
+    s = LBM(44, 12, 10, storage="f32", kernel="tile")   # nx not a multiple of 8
+    with pytest.raises(WTError):
+        s.step_forces(1)
+    s = LBM(40, 12, 10, storage="f32", kernel="tile")
+    apply_case(s, sphere=(20.0, 6.0, 5.0, 3.0), ground=True, roadVel=0.02)
+    s.set_params(moving_walls=1)
+    with pytest.raises(WTError):
+        s.step_forces(1)
+
+
 def test_pair_kernel_conditions(both):
     from windtunnel_b200 import WTError
     LBM, _ = both

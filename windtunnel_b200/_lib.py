@@ -42,6 +42,7 @@ WT_KERNEL_X2 = 5
 WT_KERNEL_TMA = 6
 WT_KERNEL_LEAN = 7
 WT_KERNEL_PAIR = 8
+WT_KERNEL_TILE = 9
 
 WT_ROUND_NEAREST = 0
 WT_ROUND_STOCHASTIC = 1

@@ -88,7 +88,7 @@ int check_params(const wt_params* p) {
   if (p->trt && !(p->lambda > 0)) return WT_ERR_ARG;
   if (p->side_bc != WT_SIDE_EQ && p->side_bc != WT_SIDE_FREESLIP) return WT_ERR_ARG;
   if (p->math != WT_MATH_FAST && p->math != WT_MATH_EXACT) return WT_ERR_ARG;
-  if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_PAIR) return WT_ERR_ARG;
+  if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_TILE) return WT_ERR_ARG;
   if (p->f16_rounding != WT_ROUND_NEAREST && p->f16_rounding != WT_ROUND_STOCHASTIC)
     return WT_ERR_ARG;
   if (p->reserved != 0) return WT_ERR_ARG;
@@ -170,13 +170,13 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
 // direction block starts on a 16-byte boundary.
 bool staged_ok(const wt_lattice* h) { return h->nx % (int)(16 / h->elem) == 0; }
 
-enum class Path { Direct, Staged, Vector, Pipe, X2, Tma, Pbb, Lean, Pair };
+enum class Path { Direct, Staged, Vector, Pipe, X2, Tma, Pbb, Lean, Pair, Tile };
 
 template <class S, class L, class LS, class LV, class LP, class LX, class LT, class LB, class LL,
-          class LH>
+          class LH, class LI>
 void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged, LV launch_vec,
                LP launch_pipe, LX launch_x2, LT launch_tma, LB launch_pbb, LL launch_lean,
-               LH launch_pair, double* forces_dev) {
+               LH launch_pair, LI launch_tile, double* forces_dev) {
   wt::StepArgs<S> a = make_args<S>(h);
   const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
   const bool wide = 19 * h->n >= (1LL << 31);
@@ -198,6 +198,7 @@ void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged,
         case Path::Pbb: launch_pbb(a, grid, wide, h->stream); break;
         case Path::Lean: launch_lean(a, grid, wide, h->stream); break;
         case Path::Pair: launch_pair(a, grid, wide, h->stream); break;
+        case Path::Tile: launch_tile(a, grid, wide, h->stream); break;
         default: launch(a, grid, wide, h->stream); break;
       }
       h->launches++;
@@ -244,6 +245,10 @@ bool lean_ok(const wt_lattice* h) {
 bool pair_ok(const wt_lattice* h) {
   return h->storage == WT_STORE_F16DEV && lean_ok(h) && h->nx % 2 == 0;
 }
+
+// True when the shared-memory tile kernel can run: the lean kernel's
+// conditions and nx a multiple of 8 (16-byte row vectors for either storage).
+bool tile_ok(const wt_lattice* h) { return lean_ok(h) && h->nx % 8 == 0; }
 
 // True when the TMA tile kernel can run.
 bool tma_ok(const wt_lattice* h) {
@@ -708,6 +713,13 @@ int select_path(wt_lattice* h, Path* out) {
                     "buffers under 2 GiB and stationary walls");
       path = Path::Pair;
       break;
+    case WT_KERNEL_TILE:
+      if (!tile_ok(h))
+        return fail(h, WT_ERR_UNSUPPORTED,
+                    "the tile kernel needs the float32 collision, nx a multiple of 8, buffers "
+                    "under 2 GiB and stationary walls");
+      path = Path::Tile;
+      break;
     case WT_KERNEL_AUTO:
       path = auto_path(h);
       break;
@@ -727,23 +739,23 @@ void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* forces_dev) {
                                   wt::launch_staged_f32_exact, no_vec<float>, no_vec<float>,
                                   no_vec<float>, no_tma<float>, wt::launch_pbb_f32_exact,
                                   wt::launch_step_f32_exact, wt::launch_step_f32_exact,
-                                  forces_dev);
+                                  wt::launch_step_f32_exact, forces_dev);
       else run_steps<float>(h, nsteps, path, wt::launch_step_f32_fast, wt::launch_staged_f32_fast,
                             wt::launch_vec_f32, wt::launch_pipe_f32, wt::launch_x2_f32,
                             wt::launch_tma_f32, wt::launch_pbb_f32_fast, wt::launch_lean_f32,
-                            wt::launch_lean_f32, forces_dev);
+                            wt::launch_lean_f32, wt::launch_tile_f32, forces_dev);
       break;
     case WT_STORE_F16DEV:
       run_steps<__half>(h, nsteps, path, wt::launch_step_f16_fast, wt::launch_staged_f16_fast,
                         wt::launch_vec_f16, wt::launch_pipe_f16, wt::launch_x2_f16,
                         wt::launch_tma_f16, wt::launch_pbb_f16_fast, wt::launch_lean_f16,
-                        wt::launch_pair_f16, forces_dev);
+                        wt::launch_pair_f16, wt::launch_tile_f16, forces_dev);
       break;
     default:
       run_steps<double>(h, nsteps, path, wt::launch_step_f64_exact, wt::launch_staged_f64_exact,
                         no_vec<double>, no_vec<double>, no_vec<double>, no_tma<double>,
                         wt::launch_pbb_f64_exact, wt::launch_step_f64_exact,
-                        wt::launch_step_f64_exact, forces_dev);
+                        wt::launch_step_f64_exact, wt::launch_step_f64_exact, forces_dev);
       break;
   }
 }

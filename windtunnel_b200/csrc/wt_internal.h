@@ -105,6 +105,8 @@ void launch_adj_f64(const StepArgs<double>& a, const double* Tn, double* Tc, dou
 void launch_lean_f32(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
 void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
 void launch_pair_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_tile_f32(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_tile_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
 
 // Software-pipelined step launchers, float32 collision.
 void launch_pipe_f32(const StepArgs<float>& a, bool wide, cudaStream_t s);

@@ -10,6 +10,7 @@
 #include "wt_pbb.cuh"
 #include "wt_lean.cuh"
 #include "wt_h2.cuh"
+#include "wt_tile.cuh"
 
 #include <algorithm>
 
@@ -55,6 +56,14 @@ void launch_lean_f32(const StepArgs<float>& a, dim3 grid, bool, cudaStream_t s) 
 
 void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool, cudaStream_t s) {
   k_step_lean<__half><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+void launch_tile_f32(const StepArgs<float>& a, dim3 grid, bool, cudaStream_t s) {
+  k_step_tile<float><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+void launch_tile_f16(const StepArgs<__half>& a, dim3 grid, bool, cudaStream_t s) {
+  k_step_tile<__half><<<grid, STEP_BX, 0, s>>>(a);
 }
 
 void launch_pair_f16(const StepArgs<__half>& a, dim3, bool, cudaStream_t s) {
