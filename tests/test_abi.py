@@ -64,3 +64,50 @@ def test_null_handle_is_an_argument_error(wt_lib):
     assert wt_lib.wt_step(None, 1, None) == _lib.WT_ERR_ARG
     assert wt_lib.wt_reset(None) == _lib.WT_ERR_ARG
     assert wt_lib.wt_destroy(None) == _lib.WT_OK
+
+
+def test_binding_constants_match_the_header():
+    """Every WT_* enumerator of include/wt.h has the same value in the ctypes
+    binding (a drifted constant would select the wrong kernel or storage)."""
+    import re
+
+    from windtunnel_b200 import _lib as W
+    text = (ROOT / "include" / "wt.h").read_text()
+    body = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    found = dict(re.findall(r"\b(WT_[A-Z0-9_]+)\s*=\s*(-?\d+)", body))
+    assert len(found) > 20
+    for name, value in found.items():
+        assert hasattr(W, name), name
+        assert getattr(W, name) == int(value), name
+
+
+def test_binding_structs_match_the_header(tmp_path):
+    """The ctypes structs have the C layout of include/wt.h (sizes and field
+    offsets, compiled with the host C compiler)."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    from windtunnel_b200 import _lib as W
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    structs = ["wt_params", "wt_body_stats", "wt_adj_cfg", "wt_adj_stats", "wt_voxel_info"]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "wt.h"', "int main(void) {"]
+    for s in structs:
+        lines.append(f'  printf("{s} %zu\\n", sizeof({s}));')
+        for f, _ in getattr(W, s)._fields_:
+            cf = f[:-1] if f.endswith("_") else f   # lambda_ is the C field lambda
+            lines.append(f'  printf("{s}.{f} %zu\\n", offsetof({s}, {cf}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True,
+                                                        text=True, check=True).stdout.split("\n") if l)
+    for s in structs:
+        cls = getattr(W, s)
+        assert int(out[s]) == ctypes.sizeof(cls), s
+        for f, _ in cls._fields_:
+            assert int(out[f"{s}.{f}"]) == getattr(cls, f).offset, (s, f)
