@@ -56,8 +56,77 @@ struct CellFw {
   T pxx, pyy, pzz, pxy, pxz, pyz, mag, R, tauEff, om, omm;
 };
 
+// The float32 form of cell_fw: the same quantities re-associated over the
+// nine opposite pairs (a, b), as the fast step collides: with s = f_a + f_b,
+// d = f_a - f_b and cv = c_a . u, the pair's symmetric and antisymmetric
+// non-equilibrium parts are sp = s/2 - w (A + 4.5 r cv^2) and
+// sm = d/2 - 3 w r cv, n_a = sp + sm, n_b = sp - sm, and the stress sums are
+// sums of 2 sp. No explicit equilibrium array.
+template <class S>
+__device__ __forceinline__ void cell_fw_pairs(const StepArgs<S>& a, CellFw<float>& c) {
+  const float* f = c.f;
+  float sp[Q], sm[Q];   // indexed by the pair's first direction (1, 3, ..., 17)
+  float s[Q], d[Q];
+#pragma unroll
+  for (int k = 1; k < Q; k += 2) {
+    s[k] = f[k] + f[k + 1];
+    d[k] = f[k] - f[k + 1];
+  }
+  const float dr = ((f[0] + s[1]) + (s[3] + s[5])) +
+                   (((s[7] + s[9]) + (s[11] + s[13])) + (s[15] + s[17]));
+  const float r = 1.0f + dr;
+  const float inv = cdiv(1.0f, r);
+  const float jx = (((d[1] + d[7]) + (d[9] + d[11])) + d[13]);
+  const float jy = (((d[3] + d[7]) - d[9]) + (d[15] + d[17]));
+  const float jz = (((d[5] + d[11]) - d[13]) + (d[15] - d[17]));
+  const float vx = jx * inv, vy = jy * inv, vz = jz * inv;
+  const float usq = vx * vx + vy * vy + vz * vz;
+  const float A = dr - r * 1.5f * usq;
+  const float r3 = 3.0f * r, r45 = 4.5f * r;
+#pragma unroll
+  for (int k = 1; k < Q; k += 2) {
+    const float cv = (float)ex(k) * vx + (float)ey(k) * vy + (float)ez(k) * vz;
+    const float w = (float)wq(k);
+    sp[k] = 0.5f * s[k] - w * (A + r45 * cv * cv);
+    sm[k] = 0.5f * d[k] - w * r3 * cv;
+    c.n[k] = sp[k] + sm[k];
+    c.n[k + 1] = sp[k] - sm[k];
+  }
+  c.n[0] = f[0] - (float)wq(0) * A;
+  const float tau0 = (float)a.tau0;
+  float om = cdiv(1.0f, tau0), tauEff = tau0;
+  c.pxx = c.pyy = c.pzz = c.pxy = c.pxz = c.pyz = c.mag = c.R = 0.0f;
+  if (a.les) {
+    c.pxx = 2.0f * (((sp[1] + sp[7]) + (sp[9] + sp[11])) + sp[13]);
+    c.pyy = 2.0f * (((sp[3] + sp[7]) + (sp[9] + sp[15])) + sp[17]);
+    c.pzz = 2.0f * (((sp[5] + sp[11]) + (sp[13] + sp[15])) + sp[17]);
+    c.pxy = 2.0f * (sp[7] - sp[9]);
+    c.pxz = 2.0f * (sp[11] - sp[13]);
+    c.pyz = 2.0f * (sp[15] - sp[17]);
+    c.mag = csqrt(2.0f * (c.pxx * c.pxx + c.pyy * c.pyy + c.pzz * c.pzz +
+                          2.0f * (c.pxy * c.pxy + c.pxz * c.pxz + c.pyz * c.pyz)));
+    const float SQ18 = (float)(18 * 1.4142135623730951);
+    c.R = csqrt(tau0 * tau0 + SQ18 * (float)a.cs2 * c.mag * inv);
+    tauEff = 0.5f * (tau0 + c.R);
+    om = cdiv(1.0f, tauEff);
+  }
+  const float omm = a.trt ? cdiv(1.0f, 0.5f + cdiv((float)a.lam, tauEff - 0.5f)) : om;
+  c.gc[0] = f[0] - om * c.n[0];
+#pragma unroll
+  for (int k = 1; k < Q; k += 2) {
+    c.gc[k] = f[k] - om * sp[k] - omm * sm[k];
+    c.gc[k + 1] = f[k + 1] - om * sp[k] + omm * sm[k];
+  }
+  c.r = r; c.inv = inv; c.jx = jx; c.jy = jy; c.jz = jz; c.vx = vx; c.vy = vy; c.vz = vz;
+  c.usq = usq; c.A = A; c.r3 = r3; c.r45 = r45; c.tauEff = tauEff; c.om = om; c.omm = omm;
+}
+
 template <class T, class S>
 __device__ __forceinline__ void cell_fw(const StepArgs<S>& a, CellFw<T>& c) {
+  if constexpr (std::is_same<T, float>::value) {
+    cell_fw_pairs(a, c);
+    return;
+  }
   const T* f = c.f;
   const T dr = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] + f[11] +
                f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
