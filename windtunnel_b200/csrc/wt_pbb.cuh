@@ -178,10 +178,85 @@ __device__ __forceinline__ void cell_fw(const StepArgs<S>& a, CellFw<T>& c) {
   c.usq = usq; c.A = A; c.r3 = r3; c.r45 = r45; c.tauEff = tauEff; c.om = om; c.omm = omm;
 }
 
+// The float32 form of cell_vjp, over the nine opposite pairs: with
+// P = nb_a + nb_b and D = nb_a - nb_b (the adjoints of the pair's
+// symmetric and antisymmetric non-equilibrium parts), the stress terms add
+// to P only, and the equilibrium's adjoint needs each pair once (c_b = -c_a).
+template <class S>
+__device__ __forceinline__ void cell_vjp_pairs(const StepArgs<S>& a, const CellFw<float>& c,
+                                               const float (&ab)[Q], float (&fb)[Q]) {
+  const float* n = c.n;
+  float P[Q], D[Q];   // indexed by the pair's first direction (1, 3, ..., 17)
+  float omb = -(ab[0] * n[0]);
+  float ommb = 0.0f;
+  const float nb0 = -(c.om * ab[0]);
+#pragma unroll
+  for (int k = 1; k < Q; k += 2) {
+    const float sp = 0.5f * (n[k] + n[k + 1]), sm = 0.5f * (n[k] - n[k + 1]);
+    const float as = ab[k] + ab[k + 1], ad = ab[k] - ab[k + 1];
+    omb -= as * sp;
+    ommb -= ad * sm;
+    P[k] = -(c.om * as);
+    D[k] = -(c.omm * ad);
+  }
+  float invb = 0.0f;
+  if (a.les) {
+    float teb;
+    if (a.trt) {
+      const float tm = c.tauEff - 0.5f;
+      teb = ommb * cdiv(c.omm * c.omm * (float)a.lam, tm * tm) - omb * (c.om * c.om);
+    } else {
+      teb = -(omb + ommb) * (c.om * c.om);
+    }
+    const float Rb = 0.5f * teb;
+    const float Xb = cdiv(Rb, 2.0f * c.R);
+    const float K = (float)(18 * 1.4142135623730951) * (float)a.cs2;
+    const float magb = Xb * K * c.inv;
+    invb += Xb * K * c.mag;
+    const float Qb = c.mag > 0.0f ? cdiv(magb, c.mag) : 0.0f;
+    const float pxxb = 4.0f * c.pxx * Qb, pyyb = 4.0f * c.pyy * Qb, pzzb = 4.0f * c.pzz * Qb;
+    const float pxyb = 8.0f * c.pxy * Qb, pxzb = 8.0f * c.pxz * Qb, pyzb = 8.0f * c.pyz * Qb;
+    P[1] += pxxb; P[3] += pyyb; P[5] += pzzb;
+    P[7] += pxxb + pyyb + pxyb; P[9] += pxxb + pyyb - pxyb;
+    P[11] += pxxb + pzzb + pxzb; P[13] += pxxb + pzzb - pxzb;
+    P[15] += pyyb + pzzb + pyzb; P[17] += pyyb + pzzb - pyzb;
+  }
+  float Ab = (float)wq(0) * (-nb0), r3b = 0.0f, r45b = 0.0f, vxb = 0.0f, vyb = 0.0f, vzb = 0.0f;
+#pragma unroll
+  for (int k = 1; k < Q; k += 2) {
+    const float E = -P[k], Dm = -D[k], w = (float)wq(k);
+    const float cv = (float)ex(k) * c.vx + (float)ey(k) * c.vy + (float)ez(k) * c.vz;
+    Ab += w * E;
+    r3b += w * cv * Dm;
+    r45b += w * (cv * cv) * E;
+    const float cvbd = w * (c.r3 * Dm + 2.0f * c.r45 * cv * E);
+    vxb += (float)ex(k) * cvbd; vyb += (float)ey(k) * cvbd; vzb += (float)ez(k) * cvbd;
+  }
+  float drb = Ab;
+  float rb = 3.0f * r3b + 4.5f * r45b - 1.5f * c.usq * Ab;
+  const float usqb = -(c.r * 1.5f * Ab);
+  vxb += 2.0f * c.vx * usqb; vyb += 2.0f * c.vy * usqb; vzb += 2.0f * c.vz * usqb;
+  invb += vxb * c.jx + vyb * c.jy + vzb * c.jz;
+  const float jxb = vxb * c.inv, jyb = vyb * c.inv, jzb = vzb * c.inv;
+  rb -= c.inv * c.inv * invb;
+  drb += rb;
+  fb[0] += ab[0] + nb0 + drb;
+#pragma unroll
+  for (int k = 1; k < Q; k += 2) {
+    const float cj = (float)ex(k) * jxb + (float)ey(k) * jyb + (float)ez(k) * jzb;
+    fb[k] += ab[k] + 0.5f * (P[k] + D[k]) + (drb + cj);
+    fb[k + 1] += ab[k + 1] + 0.5f * (P[k] - D[k]) + (drb - cj);
+  }
+}
+
 // fb += (d gc / d f)^T a for the collision of cell_fw.
 template <class T, class S>
 __device__ __forceinline__ void cell_vjp(const StepArgs<S>& a, const CellFw<T>& c, const T (&ab)[Q],
                                          T (&fb)[Q]) {
+  if constexpr (std::is_same<T, float>::value) {
+    cell_vjp_pairs(a, c, ab, fb);
+    return;
+  }
   const T* n = c.n;
   T nb[Q];
 #pragma unroll
