@@ -38,7 +38,7 @@ enum {
   WT_ERR_OOM = -2,         /* device (or pinned host) allocation failed */
   WT_ERR_CUDA = -3,        /* a CUDA runtime call failed */
   WT_ERR_DIVERGED = -4,    /* a step produced a non-finite or non-positive density */
-  WT_ERR_TIMEOUT = -5,     /* a bounded device-side wait gave up */
+  WT_ERR_TIMEOUT = -5,     /* a bounded device-side wait gave up (no current kernel waits) */
   WT_ERR_STATE = -6,       /* call not valid in the handle's current state */
   WT_ERR_UNSUPPORTED = -7  /* option combination not provided */
 };
@@ -70,40 +70,21 @@ enum {
                            layer; the plane cells still hold the equilibrium for observers */
 };
 
-/* Which step kernel runs. */
+/* Which step kernel runs. The values 2-6 and 9 named step kernels that
+ * measured slower than LEAN on B200 and were removed; they are not reused
+ * and are rejected (WT_ERR_ARG). */
 enum {
   WT_KERNEL_AUTO = 0,    /* the kernel measured fastest on B200 for the form: LEAN when it
                             can run, DIRECT otherwise */
-  WT_KERNEL_DIRECT = 1,  /* one thread per cell, populations gathered straight from HBM */
-  WT_KERNEL_STAGED = 2,  /* persistent CTAs staging the 19 pull rows with bulk copies (TMA);
-                            needs nx to be a multiple of 16 bytes / element size */
-  WT_KERNEL_VECTOR = 3,  /* two cells per thread, paired vector loads and stores with warp
-                            shuffles for the x-shifted directions; float32 collision, nx even */
-  WT_KERNEL_PIPE = 4,    /* one thread per cell for 8 z planes, the next cell's loads issued
-                            before the current cell's collision; float32 collision */
-  WT_KERNEL_X2 = 5,      /* two cells per thread with paired vector loads / stores and the
-                            collision of both cells in packed float32x2 instructions; float32
-                            collision, nx even, nearest rounding for half storage */
-  WT_KERNEL_TMA = 6,     /* persistent CTAs moving 512-cell tiles of all 19 directions through
-                            shared memory with tensor-map TMA loads and stores, packed float32x2
-                            collision; float32 collision, nx a multiple of 16 bytes / element,
-                            nearest rounding for half storage */
-  WT_KERNEL_LEAN = 7,    /* one thread per cell, 32-bit byte offsets from one pointer per cell,
+  WT_KERNEL_DIRECT = 1,  /* one thread per cell, populations gathered straight from HBM;
+                            every storage, arithmetic and boundary option */
+  WT_KERNEL_LEAN = 7     /* one thread per cell, 32-bit byte offsets from one pointer per cell,
                             the collision in storage units with approximate reciprocal / square
                             root, and for half storage on lattices whose population buffer
                             fits in twice the L2 an L2 prefetch of the populations a fixed
                             distance ahead in launch order (environment WT_PREFETCH_CELLS
                             overrides the distance at wt_create, for any lattice; 0 turns it
                             off); float32 collision, buffers under 2 GiB, stationary walls */
-  WT_KERNEL_PAIR = 8,    /* half storage: two cells per thread as packed half pairs (one
-                            32-bit load and store per direction), each cell collided as in
-                            LEAN (bit-identical results; measured slower than LEAN on B200);
-                            LEAN's conditions and an even nx */
-  WT_KERNEL_TILE = 9     /* a block's 128 cells of a row: its 19 source row segments copied
-                            into shared memory with 16-byte loads, each cell collided as in
-                            LEAN from there (bit-identical results), the outputs written back
-                            with 16-byte stores (measured slower than LEAN on B200); LEAN's
-                            conditions and nx a multiple of 8 */
 };
 
 /* Rounding of half-precision stores. Stochastic rounding draws its random
@@ -225,17 +206,17 @@ int wt_step(wt_lattice* h, int nsteps, double* forces);
  * its force-series buffers; this call keeps the force partials, the
  * per-step forces and the error word in one fixed device array of about
  * 3.2 MB instead (16384 wall segments x 8 steps of partials, 4096 steps of
- * forces), located once per device with cudaGetSymbolAddress.
- * Same results as wt_step: it runs the kernel wt_step picks for kernel
- * AUTO, DIRECT or LEAN (the one-cell-per-thread kernels).
+ * forces), whose address it looks up with cudaGetSymbolAddress on every call.
+ * Same results as wt_step: it runs the kernel wt_step picks.
  * Limits: nsteps in 0..4096 (else WT_ERR_ARG); a body with more than 16384
- * 32-cell wall segments gives WT_ERR_UNSUPPORTED; the lattice's device must
- * be the current device (else WT_ERR_STATE). The first call on a device sets
- * the scratch up and may load device code: make it (nsteps = 0 is enough)
- * before any stream capture. The scratch is shared by every lattice on the
- * device, so calls that overlap in time, from two threads or on two
- * lattices, race and give wrong forces. forces (optional) receives
- * 3*nsteps doubles as for wt_step. */
+ * 32-cell wall segments, or a solid-fraction field, gives WT_ERR_UNSUPPORTED;
+ * the lattice's device must be the current device (else WT_ERR_STATE).
+ * A call with nsteps = 0 sets up: it looks the array up and loads the device
+ * code of every step and reduction kernel a later call can launch (code
+ * loading can need device memory); make it on each device before any stream
+ * capture. The array is shared by every lattice on the device, so calls that
+ * overlap in time, from two threads or on two lattices, race and give wrong
+ * forces. forces (optional) receives 3*nsteps doubles as for wt_step. */
 int wt_step_noalloc(wt_lattice* h, int nsteps, double* forces);
 
 /* Partial bounce-back field (no reference counterpart; the differentiable

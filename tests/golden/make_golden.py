@@ -1,6 +1,8 @@
 """Generate the golden vectors of tests/golden by running the reference itself.
 
-    python tests/golden/make_golden.py [--reference /path/to/windtunnel]
+    python tests/golden/make_golden.py --reference /path/to/windtunnel
+
+(or set WT_REFERENCE_ROOT instead of passing --reference).
 
 The unmodified js/lbm.js, js/voxel.js and js/shapes.js of the reference are
 executed through tests/golden/jsmini.py (a JavaScript-subset engine; no JS
@@ -26,8 +28,6 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE))
 import jsmini  # noqa: E402
-
-DEFAULT_REF = Path("/root/reference")
 
 
 def splitmix64_draw(seed: int, k: int) -> float:
@@ -285,19 +285,28 @@ def run_geometry_cases(G, arrays, manifest):
     manifest["bodies"] = {"dims": [48, 22, 22], "cases": bodies}
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", type=Path, default=DEFAULT_REF)
-    a = ap.parse_args()
-    G = load(a.reference)
+def generate(ref: Path) -> tuple[dict, dict]:
+    """Run every case through the reference checkout at `ref`: (manifest, arrays)."""
+    G = load(ref)
     arrays: dict = {}
     manifest = {"generator": "tests/golden/make_golden.py (reference js/ run through jsmini)",
                 "solver": {}}
     for case in SOLVER_CASES:
         run_solver_case(G, case, arrays, manifest)
-        print("solver case", case["name"], "done", flush=True)
     run_geometry_cases(G, arrays, manifest)
-    print("geometry cases done", flush=True)
+    return manifest, arrays
+
+
+def main():
+    import os
+    ap = argparse.ArgumentParser()
+    env = os.environ.get("WT_REFERENCE_ROOT")
+    ap.add_argument("--reference", type=Path, required=env is None,
+                    default=Path(env) if env else None,
+                    help="root of the windtunnel checkout (holds js/lbm.js); "
+                         "default: $WT_REFERENCE_ROOT")
+    a = ap.parse_args()
+    manifest, arrays = generate(a.reference)
     np.savez_compressed(HERE / "golden.npz", **arrays)
     (HERE / "golden.json").write_text(json.dumps(manifest, indent=1, default=float))
     print("wrote", HERE / "golden.npz", (HERE / "golden.npz").stat().st_size, "bytes")

@@ -35,14 +35,7 @@ WT_SIDE_FREESLIP = 1
 
 WT_KERNEL_AUTO = 0
 WT_KERNEL_DIRECT = 1
-WT_KERNEL_STAGED = 2
-WT_KERNEL_VECTOR = 3
-WT_KERNEL_PIPE = 4
-WT_KERNEL_X2 = 5
-WT_KERNEL_TMA = 6
 WT_KERNEL_LEAN = 7
-WT_KERNEL_PAIR = 8
-WT_KERNEL_TILE = 9
 
 WT_ROUND_NEAREST = 0
 WT_ROUND_STOCHASTIC = 1

@@ -4,7 +4,6 @@
 #include <string.h>
 
 #include <algorithm>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -69,15 +68,13 @@ long long range_cells(const int rg[6]) {
 
 void free_all(wt_lattice* h) {
   void* dev[] = {h->buf[0], h->buf[1], h->flags, h->nmask, h->ux, h->uy, h->uz, h->rho, h->uwx, h->uwy,
-                 h->uwz, h->part, h->wslot, h->forces_dev, h->err_dev, h->diag_dev, h->col,
-                 h->plan, h->low, h->counters};
+                 h->uwz, h->part, h->wslot, h->forces_dev, h->err_dev, h->col, h->plan, h->low,
+                 h->counters};
   for (void* p : dev)
     if (p) cudaFree(p);
   if (h->forces_host) cudaFreeHost(h->forces_host);
   if (h->err_host) cudaFreeHost(h->err_host);
   if (h->stream) cudaStreamDestroy(h->stream);
-  delete h->tma;
-  h->tma = nullptr;
   if (h->adj_pool) cudaFree(h->adj_pool);
   h->adj_pool = nullptr;
 }
@@ -88,7 +85,8 @@ int check_params(const wt_params* p) {
   if (p->trt && !(p->lambda > 0)) return WT_ERR_ARG;
   if (p->side_bc != WT_SIDE_EQ && p->side_bc != WT_SIDE_FREESLIP) return WT_ERR_ARG;
   if (p->math != WT_MATH_FAST && p->math != WT_MATH_EXACT) return WT_ERR_ARG;
-  if (p->kernel < WT_KERNEL_AUTO || p->kernel > WT_KERNEL_TILE) return WT_ERR_ARG;
+  if (p->kernel != WT_KERNEL_AUTO && p->kernel != WT_KERNEL_DIRECT && p->kernel != WT_KERNEL_LEAN)
+    return WT_ERR_ARG;
   if (p->f16_rounding != WT_ROUND_NEAREST && p->f16_rounding != WT_ROUND_STOCHASTIC)
     return WT_ERR_ARG;
   if (p->reserved != 0) return WT_ERR_ARG;
@@ -129,7 +127,6 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
   a.uwx = h->uwx; a.uwy = h->uwy; a.uwz = h->uwz;
   a.wslot = h->wslot;
   a.err = h->err_dev;
-  a.diag = h->diag_dev;
   a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
   a.n = h->n;
   a.nxy = (long long)h->nx * h->ny;
@@ -166,56 +163,39 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
   return a;
 }
 
-// True when the staged (bulk-copy) kernel can run: every row of every
-// direction block starts on a 16-byte boundary.
-bool staged_ok(const wt_lattice* h) { return h->nx % (int)(16 / h->elem) == 0; }
+enum class Path { Direct, Lean, Pbb };
 
-enum class Path { Direct, Staged, Vector, Pipe, X2, Tma, Pbb, Lean, Pair, Tile };
+template <class S>
+using StepLaunch = void (*)(const wt::StepArgs<S>&, dim3, bool, cudaStream_t);
 
-template <class S, class L, class LS, class LV, class LP, class LX, class LT, class LB, class LL,
-          class LH, class LI>
-void run_steps(wt_lattice* h, int nsteps, Path path, L launch, LS launch_staged, LV launch_vec,
-               LP launch_pipe, LX launch_x2, LT launch_tma, LB launch_pbb, LL launch_lean,
-               LH launch_pair, LI launch_tile, double* forces_dev) {
+// nsteps steps of one kernel: the force partials of up to `chunk` steps go to
+// `part` (one block of slots per step) and are reduced into forces_dev once
+// per chunk; error bits go to `err`.
+template <class S>
+void run_steps(wt_lattice* h, int nsteps, StepLaunch<S> launch, double* part, double* forces_dev,
+               unsigned* err, int chunk_max) {
   wt::StepArgs<S> a = make_args<S>(h);
+  a.err = err;
   const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
   const bool wide = 19 * h->n >= (1LL << 31);
   const size_t stride = 3 * (size_t)h->nslots;
   for (int done = 0; done < nsteps;) {
-    const int chunk = std::min(kChunk, nsteps - done);
+    const int chunk = std::min(chunk_max, nsteps - done);
     for (int s = 0; s < chunk; s++) {
       a.F = (const S*)h->buf[h->parity];
       a.G = (S*)h->buf[h->parity ^ 1];
-      a.part = h->part + (size_t)s * stride;
+      a.part = part + (size_t)s * stride;
       a.write_fields = (done + s == nsteps - 1) ? 1 : 0;
       a.sr_seed = (unsigned)((uint64_t)(h->steps + done + s) * 0x9E3779B97F4A7C15ULL >> 32);
-      switch (path) {
-        case Path::Staged: launch_staged(a, h->stream); break;
-        case Path::Vector: launch_vec(a, wide, h->stream); break;
-        case Path::Pipe: launch_pipe(a, wide, h->stream); break;
-        case Path::X2: launch_x2(a, wide, h->stream); break;
-        case Path::Tma: launch_tma(a, *h->tma, h->parity, h->stream); break;
-        case Path::Pbb: launch_pbb(a, grid, wide, h->stream); break;
-        case Path::Lean: launch_lean(a, grid, wide, h->stream); break;
-        case Path::Pair: launch_pair(a, grid, wide, h->stream); break;
-        case Path::Tile: launch_tile(a, grid, wide, h->stream); break;
-        default: launch(a, grid, wide, h->stream); break;
-      }
+      launch(a, grid, wide, h->stream);
       h->launches++;
       h->parity ^= 1;
     }
-    wt::launch_force_reduce(h->part, (unsigned)h->nslots, chunk, forces_dev + 3 * (size_t)done,
+    wt::launch_force_reduce(part, (unsigned)h->nslots, chunk, forces_dev + 3 * (size_t)done,
                             h->stream);
     h->launches++;
     done += chunk;
   }
-}
-
-// True when the two-cells-per-thread packed kernel can run.
-bool x2_ok(const wt_lattice* h) {
-  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
-  const bool sr = h->storage == WT_STORE_F16DEV && h->p.f16_rounding == WT_ROUND_STOCHASTIC;
-  return !exact && !sr && h->nx % 2 == 0;
 }
 
 bool lean_ok(const wt_lattice* h);
@@ -223,9 +203,8 @@ bool lean_ok(const wt_lattice* h);
 // The kernel WT_KERNEL_AUTO runs, the fastest measured on B200 for the form
 // (256x128x128 channel): the lean kernel where it can run (float32 36.7k
 // MLUPS against 33.3k for the direct kernel; half, with its L2 prefetch,
-// 44.3k against 37.2k, and 39.7k for the pair kernel), the direct kernel
-// otherwise (exact collision, float64, moving walls, buffers of 2^31 bytes
-// or more).
+// 44.3k against 37.2k), the direct kernel otherwise (exact collision,
+// float64, moving walls, buffers of 2^31 bytes or more).
 Path auto_path(const wt_lattice* h) {
   if (lean_ok(h)) return Path::Lean;
   return Path::Direct;
@@ -240,33 +219,10 @@ bool lean_ok(const wt_lattice* h) {
   return !exact && !h->p.moving_walls && 19 * h->n * (long long)h->elem < (1LL << 31);
 }
 
-// True when the half-pair kernel can run: the lean kernel's conditions, half
-// storage and an even nx (32-bit pair accesses).
-bool pair_ok(const wt_lattice* h) {
-  return h->storage == WT_STORE_F16DEV && lean_ok(h) && h->nx % 2 == 0;
-}
-
-// True when the shared-memory tile kernel can run: the lean kernel's
-// conditions and nx a multiple of 8 (16-byte row vectors for either storage).
-bool tile_ok(const wt_lattice* h) { return lean_ok(h) && h->nx % 8 == 0; }
-
-// True when the TMA tile kernel can run.
-bool tma_ok(const wt_lattice* h) {
-  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
-  const bool sr = h->storage == WT_STORE_F16DEV && h->p.f16_rounding == WT_ROUND_STOCHASTIC;
-  return !exact && !sr && h->tma != nullptr;
-}
-
-template <class S>
-void no_tma(const wt::StepArgs<S>&, const wt::TmaMaps&, int, cudaStream_t) {}
-
 int select_path(wt_lattice* h, Path* out);
-void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* forces_dev);
-int check_err_word(wt_lattice* h);
-
-// No vector / pipe kernel exists for the float64 collision; this stands in their slots.
-template <class S>
-void no_vec(const wt::StepArgs<S>&, bool, cudaStream_t) {}
+void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* part, double* forces_dev,
+                    unsigned* err, int chunk);
+int check_err_word(wt_lattice* h, unsigned word);
 
 // Assign a force-partial slot to every 32-cell segment that holds a
 // near-wall cell (js/lbm.js:334-359 only accumulates there) and size the
@@ -393,7 +349,6 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
   for (float** p : fl) ok = ok && cudaMalloc((void**)p, sizeof(float) * (size_t)n) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->wslot, sizeof(int) * (size_t)h->nsegs) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->err_dev, sizeof(unsigned)) == cudaSuccess;
-  ok = ok && cudaMalloc((void**)&h->diag_dev, 4 * sizeof(long long)) == cudaSuccess;
   ok = ok && cudaMallocHost((void**)&h->err_host, sizeof(unsigned)) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->col, (size_t)ny * nz) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->plan, (size_t)nx * nz) == cudaSuccess;
@@ -420,14 +375,6 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
     free_all(h);
     delete h;
     return WT_ERR_CUDA;
-  }
-  if (wt::tma_supported(storage, nx)) {
-    // tensor maps of the TMA tile kernel over both population buffers (they never move)
-    h->tma = new wt::TmaMaps();
-    if (!wt::make_tma_maps(storage, h->buf, nx, ny, nz, h->tma)) {
-      delete h->tma;
-      h->tma = nullptr;
-    }
   }
   *out = h;
   return WT_OK;
@@ -633,11 +580,10 @@ int wt_step(wt_lattice* h, int nsteps, double* forces) {
   int c = grow_forces(h, nsteps);
   if (c != WT_OK) return c;
   WT_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(unsigned), h->stream));
-  WT_CUDA(h, cudaMemsetAsync(h->diag_dev, 0, 4 * sizeof(long long), h->stream));
   Path path = Path::Direct;
   c = select_path(h, &path);
   if (c != WT_OK) return c;
-  dispatch_steps(h, nsteps, path, h->forces_dev);
+  dispatch_steps(h, nsteps, path, h->part, h->forces_dev, h->err_dev, kChunk);
   WT_CUDA(h, cudaGetLastError());
   WT_CUDA(h, cudaMemcpyAsync(h->forces_host, h->forces_dev, sizeof(double) * 3 * (size_t)nsteps,
                              cudaMemcpyDeviceToHost, h->stream));
@@ -648,7 +594,7 @@ int wt_step(wt_lattice* h, int nsteps, double* forces) {
   const double* last = h->forces_host + 3 * (size_t)(nsteps - 1);
   h->force[0] = last[0]; h->force[1] = last[1]; h->force[2] = last[2];
   if (forces) memcpy(forces, h->forces_host, sizeof(double) * 3 * (size_t)nsteps);
-  return check_err_word(h);
+  return check_err_word(h, *h->err_host);
 }
 
 }  // extern "C"
@@ -657,9 +603,6 @@ namespace {
 
 // The kernel a wt_step call runs, from the handle's parameters.
 int select_path(wt_lattice* h, Path* out) {
-  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
-  const bool vec_ok = !exact && h->nx % 2 == 0;
-  Path path = Path::Direct;
   if (h->sfrac) {
     if (h->p.kernel != WT_KERNEL_AUTO && h->p.kernel != WT_KERNEL_DIRECT)
       return fail(h, WT_ERR_UNSUPPORTED,
@@ -667,58 +610,14 @@ int select_path(wt_lattice* h, Path* out) {
     *out = Path::Pbb;
     return WT_OK;
   }
+  Path path = Path::Direct;
   switch (h->p.kernel) {
-    case WT_KERNEL_STAGED:
-      if (!staged_ok(h))
-        return fail(h, WT_ERR_UNSUPPORTED, "the staged kernel needs nx to be a multiple of " +
-                                               std::to_string(16 / h->elem));
-      path = Path::Staged;
-      break;
-    case WT_KERNEL_VECTOR:
-      if (!vec_ok)
-        return fail(h, WT_ERR_UNSUPPORTED,
-                    "the vector kernel needs the float32 collision and an even nx");
-      path = Path::Vector;
-      break;
-    case WT_KERNEL_PIPE:
-      if (exact)
-        return fail(h, WT_ERR_UNSUPPORTED, "the pipe kernel runs the float32 collision only");
-      path = Path::Pipe;
-      break;
-    case WT_KERNEL_X2:
-      if (!x2_ok(h))
-        return fail(h, WT_ERR_UNSUPPORTED,
-                    "the x2 kernel needs the float32 collision, an even nx and nearest "
-                    "rounding for half storage");
-      path = Path::X2;
-      break;
-    case WT_KERNEL_TMA:
-      if (!tma_ok(h))
-        return fail(h, WT_ERR_UNSUPPORTED,
-                    "the TMA kernel needs the float32 collision, nx a multiple of 16 bytes / "
-                    "element (4 float32, 8 half) and nearest rounding for half storage");
-      path = Path::Tma;
-      break;
     case WT_KERNEL_LEAN:
       if (!lean_ok(h))
         return fail(h, WT_ERR_UNSUPPORTED,
                     "the lean kernel needs the float32 collision, buffers under 2 GiB "
                     "and stationary walls");
       path = Path::Lean;
-      break;
-    case WT_KERNEL_PAIR:
-      if (!pair_ok(h))
-        return fail(h, WT_ERR_UNSUPPORTED,
-                    "the pair kernel needs half storage, the float32 collision, an even nx, "
-                    "buffers under 2 GiB and stationary walls");
-      path = Path::Pair;
-      break;
-    case WT_KERNEL_TILE:
-      if (!tile_ok(h))
-        return fail(h, WT_ERR_UNSUPPORTED,
-                    "the tile kernel needs the float32 collision, nx a multiple of 8, buffers "
-                    "under 2 GiB and stationary walls");
-      path = Path::Tile;
       break;
     case WT_KERNEL_AUTO:
       path = auto_path(h);
@@ -730,53 +629,54 @@ int select_path(wt_lattice* h, Path* out) {
   return WT_OK;
 }
 
+template <class S>
+StepLaunch<S> pick(Path path, StepLaunch<S> direct, StepLaunch<S> lean, StepLaunch<S> pbb) {
+  switch (path) {
+    case Path::Lean: return lean;
+    case Path::Pbb: return pbb;
+    default: return direct;
+  }
+}
+
 // Run nsteps steps of the chosen kernel; per-step forces land in forces_dev.
-void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* forces_dev) {
+void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* part, double* forces_dev,
+                    unsigned* err, int chunk) {
   const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
   switch (h->storage) {
     case WT_STORE_F32:
-      if (exact) run_steps<float>(h, nsteps, path, wt::launch_step_f32_exact,
-                                  wt::launch_staged_f32_exact, no_vec<float>, no_vec<float>,
-                                  no_vec<float>, no_tma<float>, wt::launch_pbb_f32_exact,
-                                  wt::launch_step_f32_exact, wt::launch_step_f32_exact,
-                                  wt::launch_step_f32_exact, forces_dev);
-      else run_steps<float>(h, nsteps, path, wt::launch_step_f32_fast, wt::launch_staged_f32_fast,
-                            wt::launch_vec_f32, wt::launch_pipe_f32, wt::launch_x2_f32,
-                            wt::launch_tma_f32, wt::launch_pbb_f32_fast, wt::launch_lean_f32,
-                            wt::launch_lean_f32, wt::launch_tile_f32, forces_dev);
+      if (exact)
+        run_steps<float>(h, nsteps,
+                         pick<float>(path, wt::launch_step_f32_exact, wt::launch_step_f32_exact,
+                                     wt::launch_pbb_f32_exact),
+                         part, forces_dev, err, chunk);
+      else
+        run_steps<float>(h, nsteps,
+                         pick<float>(path, wt::launch_step_f32_fast, wt::launch_lean_f32,
+                                     wt::launch_pbb_f32_fast),
+                         part, forces_dev, err, chunk);
       break;
     case WT_STORE_F16DEV:
-      run_steps<__half>(h, nsteps, path, wt::launch_step_f16_fast, wt::launch_staged_f16_fast,
-                        wt::launch_vec_f16, wt::launch_pipe_f16, wt::launch_x2_f16,
-                        wt::launch_tma_f16, wt::launch_pbb_f16_fast, wt::launch_lean_f16,
-                        wt::launch_pair_f16, wt::launch_tile_f16, forces_dev);
+      run_steps<__half>(h, nsteps,
+                        pick<__half>(path, wt::launch_step_f16_fast, wt::launch_lean_f16,
+                                     wt::launch_pbb_f16_fast),
+                        part, forces_dev, err, chunk);
       break;
     default:
-      run_steps<double>(h, nsteps, path, wt::launch_step_f64_exact, wt::launch_staged_f64_exact,
-                        no_vec<double>, no_vec<double>, no_vec<double>, no_tma<double>,
-                        wt::launch_pbb_f64_exact, wt::launch_step_f64_exact,
-                        wt::launch_step_f64_exact, wt::launch_step_f64_exact, forces_dev);
+      run_steps<double>(h, nsteps,
+                        pick<double>(path, wt::launch_step_f64_exact, wt::launch_step_f64_exact,
+                                     wt::launch_pbb_f64_exact),
+                        part, forces_dev, err, chunk);
       break;
   }
 }
 
-// Status of the error word the last steps left in h->err_host.
-int check_err_word(wt_lattice* h) {
-  if (*h->err_host & 4u)
-    return fail(h, WT_ERR_TIMEOUT, "a staged copy did not complete within its wait budget");
-  if (*h->err_host & 8u) {
-    long long d[4] = {0, 0, 0, 0};
-    cudaMemcpy(d, h->diag_dev, sizeof(d), cudaMemcpyDeviceToHost);
-    return fail(h, WT_ERR_STATE,
-                std::string("a staged row ") + (d[0] == 2 ? "store" : "load") +
-                    " would have been misaligned or left its buffer and was skipped (direction " +
-                    std::to_string(d[1]) + ", unit " + std::to_string(d[2]) + ", element offset " +
-                    std::to_string(d[3]) + ")");
-  }
-  if (*h->err_host & 2u)
+// Status of an error word the steps left: bit 1 (a near-wall warp without a
+// force slot) and bit 0 (a non-finite or non-positive density).
+int check_err_word(wt_lattice* h, unsigned word) {
+  if (word & 2u)
     return fail(h, WT_ERR_STATE, "a near-wall warp had no force slot (occupancy changed "
                                  "without voxelize)");
-  if (*h->err_host & 1u)
+  if (word & 1u)
     return fail(h, WT_ERR_DIVERGED, "a step produced a non-finite or non-positive density");
   return WT_OK;
 }
@@ -1112,10 +1012,18 @@ int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_ad
   T* Tbuf[2] = {(T*)mem.carve(tsz), (T*)mem.carve(tsz)};
   double* ds = (double*)mem.carve(sz_ds);
   double* fdev = (double*)mem.carve(sz_f);
-  cudaEvent_t e0, e1, e2;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventCreate(&e2);
+  // the sweep timers, destroyed on every return path
+  struct Events {
+    cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+    Events() {
+      for (cudaEvent_t& x : e) cudaEventCreate(&x);
+    }
+    ~Events() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  cudaEvent_t e0 = ev.e[0], e1 = ev.e[1], e2 = ev.e[2];
   WT_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(unsigned), h->stream));
   const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
   const bool wide = 19 * h->n >= (1LL << 31);
@@ -1124,7 +1032,7 @@ int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_ad
   for (int k = 0; k + 1 < ncp; k++) {
     WT_CUDA(h, cudaMemcpyAsync(cps + (size_t)k * pel, h->buf[h->parity], pop,
                                cudaMemcpyDeviceToDevice, h->stream));
-    dispatch_steps(h, C, Path::Pbb, fdev + 3 * (size_t)k * C);
+    dispatch_steps(h, C, Path::Pbb, h->part, fdev + 3 * (size_t)k * C, h->err_dev, kChunk);
   }
   const int tl = (ncp - 1) * C, nl = N - tl;   // the last segment
   {
@@ -1191,9 +1099,6 @@ int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_ad
   float fwd_ms = 0, bwd_ms = 0;
   cudaEventElapsedTime(&fwd_ms, e0, e1);
   cudaEventElapsedTime(&bwd_ms, e1, e2);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(e2);
   double J = 0;
   for (int t = N - W; t < N; t++) J += fh[3 * (size_t)t + cfg.component];
   J /= W;
@@ -1209,7 +1114,7 @@ int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_ad
     st->checkpoints = ncp;
     st->segment = C;
   }
-  return check_err_word(h);
+  return check_err_word(h, *h->err_host);
 }
 
 }  // namespace
@@ -1261,69 +1166,33 @@ extern "C" int wt_adjoint(wt_lattice* h, const wt_adj_cfg* cfg, double* dJds, wt
 // while they run, such as a host whose own memory pool has already claimed
 // the device's memory, or a host stepping inside a frame loop that must not
 // stall (cudaMalloc / cudaFree may synchronise the whole device). wt_step
-// may grow its force series buffers
-// (cudaMalloc / cudaMallocHost); this entry point instead keeps the force
-// partials, the per-step forces and the error words in one fixed device
-// array declared below, found once per device with cudaGetSymbolAddress.
+// may grow its force series buffers (cudaMalloc / cudaMallocHost); this entry
+// point instead keeps the force partials, the per-step forces and the error
+// word in one fixed device array declared below, whose address is looked up
+// with cudaGetSymbolAddress on every call (a lookup allocates nothing once
+// the module is loaded, and stays right after a device reset).
 namespace {
 
 constexpr int kNaSlots = 16384;     // force-partial slots (32-cell segments next to a wall)
 constexpr int kNaChunk = 8;         // steps whose partials are reduced together
 constexpr int kNaMaxSteps = 4096;   // steps per call
-constexpr int kNaMaxDevices = 64;
 constexpr size_t kNaPartBytes = sizeof(double) * 3 * (size_t)kNaSlots * kNaChunk;   // 3 MiB
 constexpr size_t kNaForceBytes = sizeof(double) * 3 * (size_t)kNaMaxSteps;          // 96 KiB
 constexpr size_t kNaErrOffset = kNaPartBytes + kNaForceBytes;
-constexpr size_t kNaBytes = kNaErrOffset + 256;   // error word, then 4 diagnostic words
+constexpr size_t kNaBytes = kNaErrOffset + 256;   // error word and padding
 
-// The scratch: partials | forces | error word (4 B, 8 B pad) | diagnostics (32 B).
+// The scratch: partials | forces | error word.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
 
-std::mutex g_na_mu;
-unsigned char* g_na_ptr[kNaMaxDevices] = {};
-
-// Device address of the scratch on `dev`, which must be the current device.
-// The first call on a device may load the module's device code, so it must
-// not happen while a stream is being captured.
-int noalloc_scratch(wt_lattice* h, int dev, unsigned char** out) {
-  if (dev < 0 || dev >= kNaMaxDevices) return fail(h, WT_ERR_UNSUPPORTED, "device index too large");
-  std::lock_guard<std::mutex> lock(g_na_mu);
-  if (!g_na_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGetSymbolAddress(noalloc scratch)");
-    g_na_ptr[dev] = (unsigned char*)p;
-  }
-  *out = g_na_ptr[dev];
+// Device address of the scratch on the current device. The first lookup on a
+// device may load the module's device code, so it must not happen while a
+// stream is being captured.
+int noalloc_scratch(wt_lattice* h, unsigned char** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaGetSymbolAddress(noalloc scratch)");
+  *out = (unsigned char*)p;
   return WT_OK;
-}
-
-template <class S, class L>
-void run_steps_noalloc(wt_lattice* h, int nsteps, L launch, double* part, double* forces,
-                       unsigned* err, long long* diag) {
-  wt::StepArgs<S> a = make_args<S>(h);
-  a.err = err;
-  a.diag = diag;
-  const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
-  const bool wide = 19 * h->n >= (1LL << 31);
-  const size_t stride = 3 * (size_t)h->nslots;
-  for (int done = 0; done < nsteps;) {
-    const int chunk = std::min(kNaChunk, nsteps - done);
-    for (int s = 0; s < chunk; s++) {
-      a.F = (const S*)h->buf[h->parity];
-      a.G = (S*)h->buf[h->parity ^ 1];
-      a.part = part + (size_t)s * stride;
-      a.write_fields = (done + s == nsteps - 1) ? 1 : 0;
-      a.sr_seed = (unsigned)((uint64_t)(h->steps + done + s) * 0x9E3779B97F4A7C15ULL >> 32);
-      launch(a, grid, wide, h->stream);
-      h->launches++;
-      h->parity ^= 1;
-    }
-    wt::launch_force_reduce(part, (unsigned)h->nslots, chunk, forces + 3 * (size_t)done,
-                            h->stream);
-    h->launches++;
-    done += chunk;
-  }
 }
 
 }  // namespace
@@ -1338,46 +1207,31 @@ extern "C" int wt_step_noalloc(wt_lattice* h, int nsteps, double* forces) {
                 "wt_step_noalloc: the body has " + std::to_string(h->nslots) +
                     " wall segments, more than the " + std::to_string(kNaSlots) +
                     " its fixed scratch holds; use wt_step");
-  if (h->p.kernel != WT_KERNEL_AUTO && h->p.kernel != WT_KERNEL_DIRECT &&
-      h->p.kernel != WT_KERNEL_LEAN)
-    return fail(h, WT_ERR_UNSUPPORTED,
-                "wt_step_noalloc runs the direct or lean kernel only (the one-cell kernels)");
   if (h->sfrac)
     return fail(h, WT_ERR_UNSUPPORTED, "wt_step_noalloc does not run partial bounce-back");
   int dev = -1;
   WT_CUDA(h, cudaGetDevice(&dev));
   if (dev != h->device)
     return fail(h, WT_ERR_STATE, "wt_step_noalloc: make the lattice's device current first");
-  unsigned char* base = nullptr;
-  int c = noalloc_scratch(h, dev, &base);
+  Path path = Path::Direct;
+  int c = select_path(h, &path);   // the kernel wt_step runs for these parameters
   if (c != WT_OK) return c;
-  if (nsteps == 0) return WT_OK;
+  unsigned char* base = nullptr;
+  c = noalloc_scratch(h, &base);
+  if (c != WT_OK) return c;
+  if (nsteps == 0) {
+    // set-up call: load every kernel a later call can launch, so that none
+    // is loaded (which can need device memory) inside a later call
+    WT_CUDA(h, wt::preload_step_kernels());
+    return WT_OK;
+  }
   double* part = (double*)base;
   double* fdev = (double*)(base + kNaPartBytes);
   unsigned* err = (unsigned*)(base + kNaErrOffset);
-  long long* diag = (long long*)(base + kNaErrOffset + 8);
-  // Only the error and diagnostic words must start at zero: every used
-  // partial slot and every force entry is written before it is read.
-  WT_CUDA(h, cudaMemsetAsync(err, 0, 8 + 4 * sizeof(long long), h->stream));
-  const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
-  Path path = Path::Direct;
-  c = select_path(h, &path);   // the kernel wt_step runs for these parameters
-  if (c != WT_OK) return c;
-  const bool lean = path == Path::Lean;
-  switch (h->storage) {
-    case WT_STORE_F32:
-      if (exact) run_steps_noalloc<float>(h, nsteps, wt::launch_step_f32_exact, part, fdev, err, diag);
-      else if (lean) run_steps_noalloc<float>(h, nsteps, wt::launch_lean_f32, part, fdev, err, diag);
-      else run_steps_noalloc<float>(h, nsteps, wt::launch_step_f32_fast, part, fdev, err, diag);
-      break;
-    case WT_STORE_F16DEV:
-      if (lean) run_steps_noalloc<__half>(h, nsteps, wt::launch_lean_f16, part, fdev, err, diag);
-      else run_steps_noalloc<__half>(h, nsteps, wt::launch_step_f16_fast, part, fdev, err, diag);
-      break;
-    default:
-      run_steps_noalloc<double>(h, nsteps, wt::launch_step_f64_exact, part, fdev, err, diag);
-      break;
-  }
+  // Only the error word must start at zero: every used partial slot and
+  // every force entry is written before it is read.
+  WT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(unsigned), h->stream));
+  dispatch_steps(h, nsteps, path, part, fdev, err, kNaChunk);
   WT_CUDA(h, cudaGetLastError());
   double last[3] = {0, 0, 0};
   unsigned errw = 0;
@@ -1390,10 +1244,5 @@ extern "C" int wt_step_noalloc(wt_lattice* h, int nsteps, double* forces) {
   WT_CUDA(h, cudaStreamSynchronize(h->stream));
   h->steps += nsteps;
   h->force[0] = last[0]; h->force[1] = last[1]; h->force[2] = last[2];
-  if (errw & 2u)
-    return fail(h, WT_ERR_STATE, "a near-wall warp had no force slot (occupancy changed "
-                                 "without voxelize)");
-  if (errw & 1u)
-    return fail(h, WT_ERR_DIVERGED, "a step produced a non-finite or non-positive density");
-  return WT_OK;
+  return check_err_word(h, errw);
 }

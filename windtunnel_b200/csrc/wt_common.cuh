@@ -2,7 +2,6 @@
 // parameter blocks shared by every kernel of libwt.so.
 #pragma once
 
-#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -114,8 +113,7 @@ struct StepArgs {
   const float* uwz;
   double* part;        // this step's force partials, 3 per warp slot
   const int* wslot;    // per warp of the grid: its partial slot, or -1 (no wall cell)
-  unsigned* err;       // bit 0: non-finite / non-positive density seen
-  long long* diag;     // first rejected staged copy: {kind, q, unit, element offset}
+  unsigned* err;       // bit 0: non-finite / non-positive density; bit 1: stale slot table
   int nx, ny, nz;
   long long n;         // nx*ny*nz
   long long nxy;       // nx*ny
@@ -153,18 +151,6 @@ __device__ __forceinline__ void prefetch_ahead(const StepArgs<S>& a, long long w
   const long long e = warp_cell0 + a.pf + a.src[lane];
   if (e >= 0 && e < 19 * a.n) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.F + e));
 }
-
-// The four tensor maps of a lattice for the TMA step kernel: loads (box of
-// (tile width + 2 * halo) x tile rows) and stores (box tile width x tile rows)
-// over population buffers A and B, dims (nx, ny, nz, 19).
-struct TmaMaps {
-  CUtensorMap ld[2];
-  CUtensorMap st[2];
-  // tile geometry: tx cells x ty rows per tile; loaded boxes bw = tx + 2h wide
-  // starting h cells left of the tile; per-direction slot pitches in shared
-  // memory (elements, 128-byte multiples); tiles per row and per plane
-  int tx, ty, bw, h, in_slot, out_slot, gx, gy;
-};
 
 // Block shape of the fused step: one thread per cell along x.
 constexpr int STEP_BX = 128;

@@ -40,8 +40,6 @@ struct wt_lattice {
   int forces_cap = 0;            // steps that fit in forces_dev / forces_host
   unsigned* err_dev = nullptr;
   unsigned* err_host = nullptr;  // pinned
-  long long* diag_dev = nullptr; // first rejected staged copy {kind, q, unit, offset}
-  wt::TmaMaps* tma = nullptr;    // tensor maps of the TMA tile kernel (host copy), or null
   double* sfrac = nullptr;       // partial bounce-back solid fraction on sbox (device), or null
   void* adj_pool = nullptr;      // device memory a wt_adjoint run with keep left for the next
   size_t adj_pool_bytes = 0;
@@ -69,21 +67,6 @@ void launch_step_f16_fast(const StepArgs<__half>& a, dim3 grid, bool wide, cudaS
 void launch_step_f32_exact(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
 void launch_step_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cudaStream_t s);
 
-// Vector (two cells per thread) step launchers, float32 collision; nx even.
-void launch_vec_f32(const StepArgs<float>& a, bool wide, cudaStream_t s);
-void launch_vec_f16(const StepArgs<__half>& a, bool wide, cudaStream_t s);
-
-// Two-cells-per-thread step launchers with the packed float32x2 collision; nx even.
-void launch_x2_f32(const StepArgs<float>& a, bool wide, cudaStream_t s);
-void launch_x2_f16(const StepArgs<__half>& a, bool wide, cudaStream_t s);
-
-// TMA tile step (tensor-map loads and stores through shared memory), float32
-// collision, float32 or half storage with nx a multiple of 16 bytes.
-bool tma_supported(int storage, int nx);
-bool make_tma_maps(int storage, void* const buf[2], int nx, int ny, int nz, TmaMaps* out);
-void launch_tma_f32(const StepArgs<float>& a, const TmaMaps& m, int ld_buf, cudaStream_t s);
-void launch_tma_f16(const StepArgs<__half>& a, const TmaMaps& m, int ld_buf, cudaStream_t s);
-
 // Partial bounce-back step (direct, one thread per cell) and one step of
 // its discrete adjoint. The adjoint arithmetic is float64 for float64
 // storage or the exact collision, float32 otherwise.
@@ -104,19 +87,12 @@ void launch_adj_f64(const StepArgs<double>& a, const double* Tn, double* Tc, dou
 // float32 collision, buffers under 2^31 bytes (wide is ignored).
 void launch_lean_f32(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
 void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
-void launch_pair_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
-void launch_tile_f32(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
-void launch_tile_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
 
-// Software-pipelined step launchers, float32 collision.
-void launch_pipe_f32(const StepArgs<float>& a, bool wide, cudaStream_t s);
-void launch_pipe_f16(const StepArgs<__half>& a, bool wide, cudaStream_t s);
-
-// Staged (bulk-copy) step launchers; need nx % (16 / sizeof(S)) == 0.
-void launch_staged_f32_fast(const StepArgs<float>& a, cudaStream_t s);
-void launch_staged_f16_fast(const StepArgs<__half>& a, cudaStream_t s);
-void launch_staged_f32_exact(const StepArgs<float>& a, cudaStream_t s);
-void launch_staged_f64_exact(const StepArgs<double>& a, cudaStream_t s);
+// Load the device code of every step and reduction kernel a wt_step call can
+// launch (cudaFuncGetAttributes on each), so that none is loaded lazily
+// inside a later call. The exact variant covers the --fmad=false unit.
+cudaError_t preload_step_kernels();
+cudaError_t preload_exact_step_kernels();
 
 // Deterministic per-step sum of the warp partials: out[3*s..3*s+2].
 void launch_force_reduce(const double* part, unsigned nslots, int nsteps, double* out,

@@ -7,7 +7,6 @@
 #include <math.h>
 
 #include "wt_internal.h"
-#include "wt_staged_launch.cuh"
 #include "wt_pbb.cuh"
 
 namespace wt {
@@ -42,12 +41,16 @@ void launch_adj_f64(const StepArgs<double>& a, const double* Tn, double* Tc, dou
   launch_adjoint<double, double>(a, Tn, Tc, ds, wJ, comp, s);
 }
 
-void launch_staged_f32_exact(const StepArgs<float>& a, cudaStream_t s) {
-  launch_staged<float, true>(a, s);
-}
-
-void launch_staged_f64_exact(const StepArgs<double>& a, cudaStream_t s) {
-  launch_staged<double, true>(a, s);
+cudaError_t preload_exact_step_kernels() {
+  cudaFuncAttributes fa;
+  const void* fns[] = {(const void*)k_step<float, true, int>, (const void*)k_step<float, true, long long>,
+                       (const void*)k_step<double, true, int>,
+                       (const void*)k_step<double, true, long long>};
+  for (const void* f : fns) {
+    const cudaError_t e = cudaFuncGetAttributes(&fa, f);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 // ---- helpers -----------------------------------------------------------------

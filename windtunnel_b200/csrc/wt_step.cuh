@@ -37,18 +37,11 @@ __device__ __forceinline__ __half2 sr_half2(float a, float b, uint32_t rbits) {
   return *reinterpret_cast<__half2*>(&d);
 }
 
-// Output writers of the collision: into a register array (direct kernel) or
-// straight into a shared-memory output tile (staged kernel).
+// Output writer of the collision: a register array of the step's outputs.
 template <class S>
 struct RegOut {
   S (&o)[Q];
   __device__ __forceinline__ void put(int q, S v) { o[q] = v; }
-};
-template <class S>
-struct TileOut {
-  S* base;      // &tile[0][t]; direction q lives at base[q * stride]
-  int stride;
-  __device__ __forceinline__ void put(int q, S v) { base[q * stride] = v; }
 };
 
 enum : int { CAT_NONE = 0, CAT_EQ = 1, CAT_KEEP = 2, CAT_FLUID = 3 };

@@ -1,42 +1,22 @@
-// wt_x2.cuh — the fused step, two cells per thread, packed float32x2 collision.
+// wt_x2.cuh — the float32 collision in the storage's scaled units, written
+// once for a scalar float (one cell) and for a packed float2 (two cells in
+// the .x and .y lanes of sm_100's add / sub / mul / fma .f32x2 instructions).
 //
-// Same semantics and per-cell rules as k_step (wt_step.cuh). Thread t of a
-// block owns the adjacent cells x0 = 2*(blockIdx.x*X2_BX + t) and x0+1 of
-// row (y, z) = (blockIdx.y, blockIdx.z); nx must be even.
-//
-// Loads. Per direction q one aligned vector load (float2 / half2) fetches
-// the pair (x0, x0+1) of the source row (y - ey, z - ez). Directions with
-// ex = +1 need (x0-1, x0): x0-1 is the upper element of the previous lane's
-// pair, taken with a warp shuffle (lane 0 loads it); ex = -1 needs
-// (x0+1, x0+2), with x0+2 from the next lane (lane 31 loads it). No load is
-// misaligned and a warp's 19 loads cover exactly its 19 source row spans.
-//
-// Arithmetic. The two cells run the collision in lockstep with sm_100's
-// packed float32 instructions (add / sub / mul / fma .f32x2): cell x0 in the
-// .x lane of every float2, cell x0+1 in .y. The collision is that of
-// collide_fast (opposite pairs carried as half sums and half differences)
-// evaluated in the storage's scaled units: a half-storage lattice holds
-// 4096 * (f - w), and the collision is written so that this scale only
-// enters through r~ = 4096 + sum(f~) (moments, equilibrium, stress and the
-// TRT update are linear in f~, and the Smagorinsky term depends on
-// |Pi|/rho, which the scale leaves unchanged), so loads and stores carry no
-// scaling multiply. Reciprocals and square roots use the approximate
-// hardware instructions (relative error ~2^-22).
-//
-// Stores. The outputs of the pair go out as one packed vector store per
-// direction (one cvt.rn.f16x2.f32 per direction for half storage). Cells that
-// are not plain fluid follow k_step's rules per lane: bounce-back and
-// free-slip directions are re-gathered before the collision (patch_raw),
-// inlet / floor / edge-plane cells store the equilibrium, solid cells keep
-// their stale populations, and the outlet column x = nx-1 takes the values
-// that column nx-2 ends up holding.
+// The collision is that of collide_fast (opposite pairs carried as half sums
+// and half differences, js/lbm.js:377-460 re-associated) evaluated in raw
+// units: a half-storage lattice holds 4096 * (f - w), and the arithmetic is
+// arranged so that this scale only enters through r~ = 4096 + sum(f~)
+// (moments, equilibrium, stress and the TRT update are linear in f~, and the
+// Smagorinsky term depends on |Pi|/rho, which the scale leaves unchanged), so
+// loads and stores carry no scaling multiply. Reciprocals and square roots
+// use the approximate hardware instructions (relative error ~2^-22).
+// patch_raw re-gathers the bounce-back and free-slip directions of one cell
+// in the same raw units.
 #pragma once
 
-#include "wt_vec.cuh"
+#include "wt_step.cuh"
 
 namespace wt {
-
-constexpr int X2_BX = 128;   // threads per block: 256 cells of one row
 
 // ---- packed float32 pairs: cell x0 in .x, cell x0+1 in .y --------------------------
 using f2 = float2;
@@ -226,194 +206,6 @@ __device__ __forceinline__ void collide_x2(const StepArgs<S>& a, f2 (&f)[Q], f2&
   WT_OUT2(1, 2) WT_OUT2(3, 4) WT_OUT2(5, 6) WT_OUT2(7, 8) WT_OUT2(9, 10) WT_OUT2(11, 12)
   WT_OUT2(13, 14) WT_OUT2(15, 16) WT_OUT2(17, 18)
 #undef WT_OUT2
-}
-
-// Source pair of direction q for the two cells of this thread, in raw units.
-template <class S, class IDX, int q>
-__device__ __forceinline__ f2 pull_pair(const S* Fp, long long srcq, int lane, bool active) {
-  using T = X2<S>;
-  using V = typename T::V;
-  const IDX base = (IDX)srcq + (IDX)ex(q);   // aligned pair (x0, x0+1) of the source row
-  V v;
-  if (active) v = *reinterpret_cast<const V*>(Fp + base);
-  else memset(&v, 0, sizeof(v));
-  if constexpr (ex(q) == 0) {
-    return T::unpack(v);
-  } else if constexpr (sizeof(S) == 4) {
-    if constexpr (ex(q) == 1) {
-      float prev = __shfl_up_sync(0xffffffffu, v.y, 1);
-      if (lane == 0 && active) prev = Fp[base - 1];
-      return make_float2(prev, v.x);
-    } else {
-      float nxt = __shfl_down_sync(0xffffffffu, v.x, 1);
-      if (lane == 31 && active) nxt = Fp[base + 2];
-      return make_float2(v.y, nxt);
-    }
-  } else {
-    unsigned w;
-    memcpy(&w, &v, 4);
-    if constexpr (ex(q) == 1) {
-      unsigned wp = __shfl_up_sync(0xffffffffu, w, 1);
-      if (lane == 0 && active) wp = (unsigned)__half_as_ushort(Fp[base - 1]) << 16;
-      const unsigned u = __byte_perm(wp, w, 0x5432);   // (prev.hi, this.lo)
-      V h;
-      memcpy(&h, &u, 4);
-      return T::unpack(h);
-    } else {
-      unsigned wn = __shfl_down_sync(0xffffffffu, w, 1);
-      if (lane == 31 && active) wn = (unsigned)__half_as_ushort(Fp[base + 2]);
-      const unsigned u = __byte_perm(w, wn, 0x5432);   // (this.hi, next.lo)
-      V h;
-      memcpy(&h, &u, 4);
-      return T::unpack(h);
-    }
-  }
-}
-
-template <class S, class IDX>
-__global__ void __launch_bounds__(X2_BX, 4) k_step_x2(const __grid_constant__ StepArgs<S> a) {
-  using T = X2<S>;
-  using V = typename T::V;
-  constexpr float SC = T::SC;
-  const int t = threadIdx.x;
-  const int lane = t & 31;
-  const int x0 = 2 * (blockIdx.x * X2_BX + t);
-  const int y = blockIdx.y, z = blockIdx.z;
-  const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const long long i0 = (long long)x0 + (long long)nx * y + a.nxy * z;
-  const bool active = x0 < nx;
-  const bool edge_row = z == 0 || z == nz - 1 || y == ny - 1;
-  double Fx = 0, Fy = 0, Fz = 0;
-  bool near_any = false;
-  S* Gi = a.G + i0;
-
-  if (edge_row) {
-    // ceiling / end planes: equilibrium for both cells (the outlet's copy of an
-    // equilibrium cell is the equilibrium)
-    if (active) {
-#pragma unroll
-      for (int q = 0; q < Q; q++) {
-        V e;
-        const S eqs[2] = {a.eq[q], a.eq[q]};
-        memcpy(&e, eqs, sizeof(e));
-        *reinterpret_cast<V*>(Gi + (IDX)a.dst[q]) = e;
-      }
-      if (a.write_fields) {
-        a.ux[i0] = a.u0f; a.uy[i0] = 0.0f; a.uz[i0] = 0.0f; a.rho[i0] = 1.0f;
-        a.ux[i0 + 1] = a.u0f; a.uy[i0 + 1] = 0.0f; a.uz[i0 + 1] = 0.0f; a.rho[i0 + 1] = 1.0f;
-      }
-    }
-    pair_force_partial(Fx, Fy, Fz, near_any, a, x0 & ~31, y, z);
-    return;
-  }
-
-  uint8_t flA = 0, flB = 0;
-  if (active) {
-    flA = a.flags[i0];
-    flB = a.flags[i0 + 1];
-  }
-  const int catA = cell_category(a, x0, y, flA);
-  const int catB = (x0 + 1 == nx - 1) ? CAT_NONE : cell_category(a, x0 + 1, y, flB);
-  const bool fluidA = active && catA == CAT_FLUID, fluidB = active && catB == CAT_FLUID;
-
-  f2 f[Q];
-  f2 r = pk(SC), vx = pk(0.0f), vy = pk(0.0f), vz = pk(0.0f);
-  if (y == 0) {
-#pragma unroll
-    for (int q = 0; q < Q; q++) f[q] = pk(0.0f);   // floor row: nothing is pulled
-  } else {
-    // interior row: vector pull of the 19 source rows (every lane takes part in the shuffles)
-    const S* Fp = a.F + i0;
-    f[0] = pull_pair<S, IDX, 0>(Fp, a.src[0], lane, active);
-    f[1] = pull_pair<S, IDX, 1>(Fp, a.src[1], lane, active);
-    f[2] = pull_pair<S, IDX, 2>(Fp, a.src[2], lane, active);
-    f[3] = pull_pair<S, IDX, 3>(Fp, a.src[3], lane, active);
-    f[4] = pull_pair<S, IDX, 4>(Fp, a.src[4], lane, active);
-    f[5] = pull_pair<S, IDX, 5>(Fp, a.src[5], lane, active);
-    f[6] = pull_pair<S, IDX, 6>(Fp, a.src[6], lane, active);
-    f[7] = pull_pair<S, IDX, 7>(Fp, a.src[7], lane, active);
-    f[8] = pull_pair<S, IDX, 8>(Fp, a.src[8], lane, active);
-    f[9] = pull_pair<S, IDX, 9>(Fp, a.src[9], lane, active);
-    f[10] = pull_pair<S, IDX, 10>(Fp, a.src[10], lane, active);
-    f[11] = pull_pair<S, IDX, 11>(Fp, a.src[11], lane, active);
-    f[12] = pull_pair<S, IDX, 12>(Fp, a.src[12], lane, active);
-    f[13] = pull_pair<S, IDX, 13>(Fp, a.src[13], lane, active);
-    f[14] = pull_pair<S, IDX, 14>(Fp, a.src[14], lane, active);
-    f[15] = pull_pair<S, IDX, 15>(Fp, a.src[15], lane, active);
-    f[16] = pull_pair<S, IDX, 16>(Fp, a.src[16], lane, active);
-    f[17] = pull_pair<S, IDX, 17>(Fp, a.src[17], lane, active);
-    f[18] = pull_pair<S, IDX, 18>(Fp, a.src[18], lane, active);
-    if (fluidA || fluidB) {
-      const bool shell = a.freeslip && (y == 1 || y == ny - 2 || z == 1 || z == nz - 2);
-      const bool nearA = fluidA && (flA & FLAG_NEAR) != 0;
-      const bool nearB = fluidB && (flB & FLAG_NEAR) != 0;
-      near_any = nearA || nearB;
-      if (fluidA && (nearA || shell)) patch_raw<S, 0>(a, i0, x0, y, z, nearA, shell, f, Fx, Fy, Fz);
-      if (fluidB && (nearB || shell))
-        patch_raw<S, 1>(a, i0 + 1, x0 + 1, y, z, nearB, shell, f, Fx, Fy, Fz);
-      collide_x2<S>(a, f, r, vx, vy, vz);
-      if ((fluidA && !(r.x > 0.0f && r.x < 3.0e38f)) || (fluidB && !(r.y > 0.0f && r.y < 3.0e38f)))
-        atomicOr(a.err, 1u);
-      if (a.mov && !a.write_fields) {
-        if (nearA) a.rho[i0] = r.x * (1.0f / SC);
-        if (nearB) a.rho[i0 + 1] = r.y * (1.0f / SC);
-      }
-    }
-  }
-
-  if (active) {
-    // lane selection: fluid -> collided, equilibrium -> eq, solid -> keep,
-    // outlet (cell B at x = nx-1) -> whatever cell A ends up holding
-    const bool eqA = catA == CAT_EQ, eqB = catB == CAT_EQ;
-    const bool keepA = catA == CAT_KEEP;
-    const bool outB = catB == CAT_NONE;
-    const bool storeA = !keepA, storeB = catB != CAT_KEEP;
-    if (storeA && storeB && !eqA && !eqB && !outB) {
-#pragma unroll
-      for (int q = 0; q < Q; q++) *reinterpret_cast<V*>(Gi + (IDX)a.dst[q]) = T::pack(f[q]);
-    } else {
-#pragma unroll
-      for (int q = 0; q < Q; q++) {
-        S sa, sb;
-        const V pv = T::pack(f[q]);
-        S two[2];
-        memcpy(two, &pv, sizeof(two));
-        sa = eqA ? a.eq[q] : two[0];
-        sb = eqB ? a.eq[q] : two[1];
-        if (outB) sb = keepA ? Gi[(IDX)a.dst[q]] : sa;
-        if (storeA && storeB) {
-          const S pair[2] = {sa, sb};
-          V o;
-          memcpy(&o, pair, sizeof(o));
-          *reinterpret_cast<V*>(Gi + (IDX)a.dst[q]) = o;
-        } else if (storeA) {
-          Gi[(IDX)a.dst[q]] = sa;
-        } else if (storeB) {
-          Gi[(IDX)a.dst[q] + 1] = sb;
-        }
-      }
-    }
-    if (a.write_fields) {
-      float ra = 1.0f, xa = a.u0f, ya = 0.0f, za = 0.0f;
-      if (fluidA) { ra = r.x * (1.0f / SC); xa = vx.x; ya = vy.x; za = vz.x; }
-      if (keepA) { ra = a.rho[i0]; xa = a.ux[i0]; ya = a.uy[i0]; za = a.uz[i0]; }
-      else { a.rho[i0] = ra; a.ux[i0] = xa; a.uy[i0] = ya; a.uz[i0] = za; }
-      if (outB) {
-        a.rho[i0 + 1] = ra; a.ux[i0 + 1] = xa; a.uy[i0 + 1] = ya; a.uz[i0 + 1] = za;
-      } else if (fluidB) {
-        a.rho[i0 + 1] = r.y * (1.0f / SC); a.ux[i0 + 1] = vx.y; a.uy[i0 + 1] = vy.y;
-        a.uz[i0 + 1] = vz.y;
-      } else if (eqB) {
-        a.rho[i0 + 1] = 1.0f; a.ux[i0 + 1] = a.u0f; a.uy[i0 + 1] = 0.0f; a.uz[i0 + 1] = 0.0f;
-      }
-    }
-  }
-  constexpr double inv_sc = 1.0 / (double)SC;   // a power of two: exact
-  pair_force_partial(Fx * inv_sc, Fy * inv_sc, Fz * inv_sc, near_any, a, x0 & ~31, y, z);
-}
-
-inline dim3 x2_grid(int nx, int ny, int nz) {
-  return dim3((unsigned)((nx + 2 * X2_BX - 1) / (2 * X2_BX)), (unsigned)ny, (unsigned)nz);
 }
 
 }  // namespace wt
