@@ -50,81 +50,26 @@ METRIC = ("MLUPS FP32 vs FP16-store at |ΔCd|<1% vs FP64; "
 BYTES_PER_CELL = {"f32": 152, "f16dev": 76, "f64": 304}
 FALLBACK_HBM_GBS = 6650.0
 
-WORKLOADS = {
-    "channel256": dict(
-        name="256x128x128 D3Q19 channel, yawed superellipsoid hull",
-        nx=256, ny=128, nz=128, u0=0.06, tau=0.5072, csm=0.1, lam=3 / 16, les=True,
-        side_bc="freeslip", body=dict(semi=(0.5, 0.1875, 0.15), exponent=2.5, res=160,
-                                      scale=80.0, yaw_deg=15.0), seed=1234, amp=1e-4,
-        accuracy_steps=10000, accuracy_window=2000),
-    "sphere128": dict(
-        name="128x64x64 D3Q19 channel, sphere r=8 at (32,32,32), Re=100 (steady wake)",
-        nx=128, ny=64, nz=64, u0=0.05, tau=0.524, csm=0.1, lam=3 / 16, les=True,
-        side_bc="freeslip", sphere=(32.0, 32.0, 32.0, 8.0), seed=1234, amp=1e-4,
-        accuracy_steps=8000, accuracy_window=1000),
-    "channel512": dict(
-        name="512x192x192 D3Q19 channel, yawed superellipsoid hull x2",
-        nx=512, ny=192, nz=192, u0=0.06, tau=0.5072, csm=0.1, lam=3 / 16, les=True,
-        side_bc="freeslip", body=dict(semi=(0.5, 0.1875, 0.15), exponent=2.5, res=160,
-                                      scale=160.0, yaw_deg=15.0), seed=1234, amp=1e-4,
-        accuracy_steps=8000, accuracy_window=2000),
-}
+from windtunnel_b200.workloads import WORKLOADS, channel_lattice  # noqa: E402
 
 
 # ---------------------------------------------------------------------------- set-up
-_GRIDS = {}
-
-
-def body_inputs(wl, on_gpu: bool = True):
-    """The benchmark body: a seeded 20000-triangle superellipsoid hull with a
-    radial bump field, oriented and length-normalised (Shapes.orient), voxelised
-    with Voxel.build at `res` cells along its length (on the GPU, or for the
-    CPU arms by the oracle's restatement, which gives the same grid bit for
-    bit), placed at scale / yaw / pos by the lookup."""
-    from windtunnel_b200.bodies import body_box, body_matrix
-    from windtunnel_b200.mesh import VoxelGrid, hull_mesh, orient, voxel_build
-    b = wl["body"]
-    key = (b["semi"], b["exponent"], b["res"], on_gpu)
-    if key not in _GRIDS:
-        tris = hull_mesh(semi=b["semi"], exponent=b["exponent"], seed=wl["seed"])
-        orient(tris, 0, 1)
-        if on_gpu:
-            _GRIDS[key] = voxel_build(tris, b["res"])
-        else:
-            from oracle.oracle import voxel_build as oracle_voxel_build
-            grid, info = oracle_voxel_build(tris, b["res"])
-            _GRIDS[key] = VoxelGrid(grid=grid, **{k: info[k] for k in (
-                "nx", "ny", "nz", "cell", "min", "inv", "ext", "centre", "bbox", "tris",
-                "solid", "openness")})
-    vg = _GRIDS[key]
-    M = body_matrix(math.radians(b["yaw_deg"]), 0.0)
-    P = [0.36 * wl["nx"], 0.5 * wl["ny"], 0.5 * wl["nz"]]
-    box = body_box(M, vg.ext, b["scale"], P)
-    return vg, M, P, box
-
-
-def setup_gpu(wl, storage, math_mode="fast"):
-    from windtunnel_b200 import LBM, sphere_box, sphere_inside
-    sim = LBM(wl["nx"], wl["ny"], wl["nz"], storage=storage, math=math_mode,
-              side_bc=wl["side_bc"])
-    sim.set_params(u0=wl["u0"], tau=wl["tau"], csm=wl["csm"], les=int(wl["les"]),
-                   **{"lambda": wl["lam"]})
-    if "sphere" in wl:
-        sim.voxelize(sphere_inside(*wl["sphere"]), sphere_box(*wl["sphere"]))
-    else:
-        vg, M, P, box = body_inputs(wl)
-        sim.voxelize_grid(vg.grid, vg.min, vg.inv, M, P, wl["body"]["scale"], box)
-    sim.init_eq_noise(wl["seed"], wl["amp"])
-    return sim
+def setup_gpu(wl, storage, math_mode="fast", kernel="auto"):
+    return channel_lattice(wl, storage, math_mode, kernel)
 
 
 def setup_oracle(wl):
-    from oracle.oracle import OracleLBM, lookup_mask
+    """The workload on the CPU oracle: the same hull voxelised by the oracle's
+    Voxel.build (bit-identical to the GPU's), the same lookup, parameters
+    and seeded state."""
+    from oracle.oracle import OracleLBM, lookup_mask, voxel_build as oracle_voxel_build
+    from windtunnel_b200.workloads import hull_triangles, placement, set_params
     o = OracleLBM(wl["nx"], wl["ny"], wl["nz"], "f32", side_bc=wl["side_bc"])
-    o.set_params(u0=wl["u0"], tau=wl["tau"], csm=wl["csm"], les=int(wl["les"]),
-                 **{"lambda": wl["lam"]})
-    vg, M, P, box = body_inputs(wl, on_gpu=False)
-    mask = lookup_mask(vg.grid, vg.min, vg.inv, M, P, wl["body"]["scale"], wl["nx"], wl["ny"],
+    set_params(o, wl)
+    b = wl["body"]
+    grid, info = oracle_voxel_build(hull_triangles(b, wl["seed"]), b["res"])
+    M, P, box = placement(wl, info["ext"])
+    mask = lookup_mask(grid, info["min"], info["inv"], M, P, b["scale"], wl["nx"], wl["ny"],
                        wl["nz"], box)
     o.voxelize_mask(box, mask)
     o.init_eq_noise(wl["seed"], wl["amp"])

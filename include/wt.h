@@ -74,17 +74,20 @@ enum {
  * measured slower than LEAN on B200 and were removed; they are not reused
  * and are rejected (WT_ERR_ARG). */
 enum {
-  WT_KERNEL_AUTO = 0,    /* the kernel measured fastest on B200 for the form: LEAN when it
-                            can run, DIRECT otherwise */
+  WT_KERNEL_AUTO = 0,    /* the kernel measured fastest on B200 for the form: PAIR for half
+                            storage when it can run, else LEAN when it can run, else DIRECT */
   WT_KERNEL_DIRECT = 1,  /* one thread per cell, populations gathered straight from HBM;
                             every storage, arithmetic and boundary option */
-  WT_KERNEL_LEAN = 7     /* one thread per cell, 32-bit byte offsets from one pointer per cell,
+  WT_KERNEL_LEAN = 7,    /* one thread per cell, 32-bit byte offsets from one pointer per cell,
                             the collision in storage units with approximate reciprocal / square
                             root, and for half storage on lattices whose population buffer
                             fits in twice the L2 an L2 prefetch of the populations a fixed
                             distance ahead in launch order (environment WT_PREFETCH_CELLS
                             overrides the distance at wt_create, for any lattice; 0 turns it
                             off); float32 collision, buffers under 2 GiB, stationary walls */
+  WT_KERNEL_PAIR = 8     /* half storage: two adjacent cells per thread, one 32-bit load and
+                            store per direction and pair, both cells collided at once in
+                            packed float32x2 instructions; LEAN's conditions and an even nx */
 };
 
 /* Rounding of half-precision stores. Stochastic rounding draws its random

@@ -57,3 +57,22 @@ def pair_average(series: np.ndarray) -> np.ndarray:
     """Average of consecutive steps, js/main.js:113-127 (cancels the odd/even oscillation)."""
     s = np.asarray(series, np.float64)
     return 0.5 * (s[1:] + s[:-1])
+
+
+def oracle_channel(wl):
+    """A benchmark channel (windtunnel_b200.workloads) on the CPU oracle: the
+    hull voxelised by the oracle's Voxel.build (bit-identical to the GPU's),
+    placed by the oracle's lookup, with the workload's parameters and seeded
+    state."""
+    from oracle.oracle import OracleLBM, lookup_mask, voxel_build
+    from windtunnel_b200.workloads import hull_triangles, placement, set_params
+    o = OracleLBM(wl["nx"], wl["ny"], wl["nz"], "f32", side_bc=wl["side_bc"])
+    set_params(o, wl)
+    b = wl["body"]
+    grid, info = voxel_build(hull_triangles(b, wl["seed"]), b["res"])
+    M, P, box = placement(wl, info["ext"])
+    mask = lookup_mask(grid, info["min"], info["inv"], M, P, b["scale"], wl["nx"], wl["ny"],
+                       wl["nz"], box)
+    o.voxelize_mask(box, mask)
+    o.init_eq_noise(wl["seed"], wl["amp"])
+    return o

@@ -10,6 +10,8 @@ Bars:
     differs) and is independent of the checkpoint interval (bit-identical);
   * the float32 adjoint of the float32 step agrees with the float64 oracle
     gradient to 1e-3 in relative L2;
+  * the half-storage adjoint agrees with the oracle's float32-storage
+    adjoint to 5e-2 in relative L2 (cosine >= 0.998);
   * the float64 GPU gradient matches central differences of the float64 GPU
     forward (eps 1e-4) to 1e-5 relative.
 """
@@ -117,6 +119,21 @@ def test_adjoint_f32_close_to_f64(wt_lib, oracle_lib):
     _, go = _oracle("f64").adjoint(N, W)
     rel_l2 = np.linalg.norm(gf - go) / np.linalg.norm(go)
     assert rel_l2 <= 1e-3, rel_l2
+
+
+def test_adjoint_f16_close_to_f32(wt_lib, oracle_lib):
+    """The half-storage adjoint (half states, float32 adjoint arithmetic; the
+    form of the 384x160x160 differentiation workload) against the oracle's
+    float32-storage adjoint: the two linearise around trajectories that
+    differ by the half rounding of every stored population."""
+    N, W = 40, 15
+    Jh, gh, st = _gpu("f16dev", math="fast").adjoint(N, W, checkpoint=6)
+    Jo, go = _oracle("f32").adjoint(N, W)
+    rel_l2 = np.linalg.norm(gh - go) / np.linalg.norm(go)
+    cos = float((gh * go).sum() / (np.linalg.norm(gh) * np.linalg.norm(go)))
+    assert abs(Jh - Jo) <= 1e-3 * abs(Jo), (Jh, Jo)
+    assert rel_l2 <= 5e-2 and cos >= 0.998, (rel_l2, cos)
+    assert st["checkpoints"] == 7
 
 
 def test_adjoint_matches_gpu_central_differences(wt_lib):

@@ -165,7 +165,7 @@ def test_fast_cfg0_drag_and_fields(both):
     assert abs(clg - clo) <= 1e-3 * abs(cdo), (clg, clo)
 
 
-@pytest.mark.parametrize("kernel", ["direct", "lean"])
+@pytest.mark.parametrize("kernel", ["direct", "lean", "pair"])
 def test_f16dev_within_tolerance(both, kernel):
     g, o = make_pair(both, (48, 24, 24), "f16dev", "fast", kernel=kernel,
                      sphere=(14.0, 12.0, 12.0, 5.0))
@@ -219,7 +219,7 @@ def test_kernels_agree(both, storage, dims):
     LBM, _ = both
     nx = dims[0]
     sims = []
-    for kernel in ("direct", "lean"):
+    for kernel in ("direct", "lean") + (("pair",) if storage == "f16dev" else ()):
         s = LBM(*dims, storage=storage, kernel=kernel, side_bc="freeslip")
         apply_case(s, sphere=(nx - 6.0, dims[1] / 2, dims[2] / 2, 3.1), side_bc="freeslip",
                    ground=True)
@@ -234,14 +234,16 @@ def test_kernels_agree(both, storage, dims):
         assert np.abs(pa - pb).max() <= (1e-6 if storage == "f32" else 1e-4)
 
 
-@pytest.mark.parametrize("kernel,moving", [("lean", False)])
+@pytest.mark.parametrize("kernel,moving", [("lean", False), ("pair", False)])
 @pytest.mark.parametrize("storage", ["f32", "f16dev"])
 @pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
 def test_kernels_agree_with_direct_at_the_outlet(both, kernel, moving, storage, side_bc):
-    """The lean kernel against the direct kernel with the special rules it
-    runs: a body touching the outlet column, a road and the side planes;
-    fields are checked on an intermediate and the last step."""
+    """The lean and pair kernels against the direct kernel with the special
+    rules they run: a body touching the outlet column, a road and the side
+    planes; fields are checked on an intermediate and the last step."""
     LBM, _ = both
+    if kernel == "pair" and storage != "f16dev":
+        pytest.skip("the pair kernel runs half storage only")
     dims = (40, 14, 12)
     out = []
     for kern in ("direct", kernel):
@@ -258,6 +260,62 @@ def test_kernels_agree_with_direct_at_the_outlet(both, kernel, moving, storage, 
     for a, b in list(zip(ua1, ub1)) + list(zip(ua2, ub2)):
         assert np.abs(a - b).max() <= (1e-6 if storage == "f32" else 2e-4)
     assert np.abs(pa - pb).max() <= (1e-6 if storage == "f32" else 1e-4)
+
+
+@pytest.mark.parametrize("dims", [(40, 14, 12), (64, 20, 18), (130, 9, 9), (136, 10, 9),
+                                  (4, 6, 6)])
+@pytest.mark.parametrize("rounding", ["nearest", "stochastic"])
+@pytest.mark.parametrize("side_bc", ["eq", "freeslip"])
+def test_pair_kernel_agrees_with_lean(both, dims, rounding, side_bc):
+    """The pair kernel (two cells per thread, packed collision) against the
+    lean kernel: a body touching the outlet column, a road, either side
+    condition, rows of one, part of one and several 128-cell blocks and the
+    smallest even row. Both collide in float32 with different
+    re-associations, so the two agree to the half-storage tolerance of the
+    other kernel comparisons; the inlet column holds the equilibrium and the
+    outlet column an exact copy of column nx-2 in both."""
+    LBM, _ = both
+    out = []
+    nx, ny, nz = dims
+    for kern in ("lean", "pair"):
+        s = LBM(*dims, storage="f16dev", kernel=kern, side_bc=side_bc)
+        s.set_params(f16_rounding=rounding)
+        sphere = (nx - 4.5, ny / 2, nz / 2, 3.3) if nx > 8 else None
+        apply_case(s, sphere=sphere, side_bc=side_bc, ground=True)
+        f1 = s.step_forces(7)
+        u1 = s.fields()
+        f2 = s.step_forces(18)
+        p = s.populations("f", "raw").reshape(19, nz, ny, nx)
+        assert np.array_equal(p[:, 1:-1, 1:-1, -1], p[:, 1:-1, 1:-1, -2])
+        out.append((np.concatenate([f1, f2]), u1, s.fields(), s.populations("f", "f32"),
+                    p[:, 1:-1, 1:-1, 0].copy()))
+    (fa, ua1, ua2, pa, ia), (fb, ub1, ub2, pb, ib) = out
+    assert np.array_equal(ia, ib)        # inlet column: the equilibrium in both
+    scale = max(np.abs(fa).max(), 1e-30)
+    assert np.abs(fa - fb).max() <= 1e-3 * scale
+    for a, b in list(zip(ua1, ub1)) + list(zip(ua2, ub2)):
+        assert np.abs(a - b).max() <= 2e-4
+    assert np.abs(pa - pb).max() <= 1e-4
+
+
+def test_pair_kernel_conditions(both):
+    from windtunnel_b200 import WTError
+    from windtunnel_b200 import _lib as W
+    LBM, _ = both
+    for dims, storage in (((41, 12, 10), "f16dev"), ((40, 12, 10), "f32")):
+        s = LBM(*dims, storage=storage, kernel="pair")
+        with pytest.raises(WTError) as e:
+            s.step_forces(1)
+        assert e.value.code == W.WT_ERR_UNSUPPORTED
+    s = LBM(40, 12, 10, storage="f16dev", kernel="pair")
+    apply_case(s, sphere=(20.0, 6.0, 5.0, 3.0), ground=True, roadVel=0.02)
+    with pytest.raises(WTError):
+        s.step_forces(1)
+    # AUTO falls back to the direct kernel with moving walls, to lean for odd nx
+    for dims, rv in (((40, 12, 10), 0.02), ((41, 12, 10), 0.0)):
+        s = LBM(*dims, storage="f16dev")
+        apply_case(s, sphere=(20.0, 6.0, 5.0, 3.0), ground=True, roadVel=rv)
+        s.step_forces(3)
 
 
 def test_lean_stochastic_rounding_agrees_with_direct(both):

@@ -36,6 +36,7 @@ WT_SIDE_FREESLIP = 1
 WT_KERNEL_AUTO = 0
 WT_KERNEL_DIRECT = 1
 WT_KERNEL_LEAN = 7
+WT_KERNEL_PAIR = 8
 
 WT_ROUND_NEAREST = 0
 WT_ROUND_STOCHASTIC = 1

@@ -85,7 +85,8 @@ int check_params(const wt_params* p) {
   if (p->trt && !(p->lambda > 0)) return WT_ERR_ARG;
   if (p->side_bc != WT_SIDE_EQ && p->side_bc != WT_SIDE_FREESLIP) return WT_ERR_ARG;
   if (p->math != WT_MATH_FAST && p->math != WT_MATH_EXACT) return WT_ERR_ARG;
-  if (p->kernel != WT_KERNEL_AUTO && p->kernel != WT_KERNEL_DIRECT && p->kernel != WT_KERNEL_LEAN)
+  if (p->kernel != WT_KERNEL_AUTO && p->kernel != WT_KERNEL_DIRECT && p->kernel != WT_KERNEL_LEAN &&
+      p->kernel != WT_KERNEL_PAIR)
     return WT_ERR_ARG;
   if (p->f16_rounding != WT_ROUND_NEAREST && p->f16_rounding != WT_ROUND_STOCHASTIC)
     return WT_ERR_ARG;
@@ -156,14 +157,21 @@ wt::StepArgs<S> make_args(wt_lattice* h) {
   a.f16_sr = p.f16_rounding == WT_ROUND_STOCHASTIC ? 1 : 0;
   double eq[19];
   wt::eq_u0_table(p.u0, eq);
-  for (int q = 0; q < 19; q++) a.eq[q] = to_store<S>(eq[q]);
+  for (int q = 0; q < 19; q++) {
+    a.eq[q] = to_store<S>(eq[q]);
+    if constexpr (sizeof(S) == 2) {
+      uint16_t b;
+      memcpy(&b, &a.eq[q], 2);
+      a.eq2[q] = (uint32_t)b | ((uint32_t)b << 16);
+    }
+  }
   a.sfrac = h->sfrac;
   for (int k = 0; k < 6; k++) a.sb[k] = h->sbox[k];
   a.pf = h->pf;   // read by the lean kernel only
   return a;
 }
 
-enum class Path { Direct, Lean, Pbb };
+enum class Path { Direct, Lean, Pbb, Pair };
 
 template <class S>
 using StepLaunch = void (*)(const wt::StepArgs<S>&, dim3, bool, cudaStream_t);
@@ -199,6 +207,7 @@ void run_steps(wt_lattice* h, int nsteps, StepLaunch<S> launch, double* part, do
 }
 
 bool lean_ok(const wt_lattice* h);
+bool pair_ok(const wt_lattice* h);
 
 // The kernel WT_KERNEL_AUTO runs, the fastest measured on B200 for the form
 // (256x128x128 channel): the lean kernel where it can run (float32 36.7k
@@ -206,6 +215,7 @@ bool lean_ok(const wt_lattice* h);
 // 44.3k against 37.2k), the direct kernel otherwise (exact collision,
 // float64, moving walls, buffers of 2^31 bytes or more).
 Path auto_path(const wt_lattice* h) {
+  if (pair_ok(h)) return Path::Pair;
   if (lean_ok(h)) return Path::Lean;
   return Path::Direct;
 }
@@ -217,6 +227,12 @@ Path auto_path(const wt_lattice* h) {
 bool lean_ok(const wt_lattice* h) {
   const bool exact = h->p.math == WT_MATH_EXACT || h->storage == WT_STORE_F64;
   return !exact && !h->p.moving_walls && 19 * h->n * (long long)h->elem < (1LL << 31);
+}
+
+// True when the half-pair kernel can run: half storage, the lean kernel's
+// conditions and an even nx (aligned 32-bit pairs of cells).
+bool pair_ok(const wt_lattice* h) {
+  return h->storage == WT_STORE_F16DEV && lean_ok(h) && h->nx % 2 == 0;
 }
 
 int select_path(wt_lattice* h, Path* out);
@@ -619,6 +635,13 @@ int select_path(wt_lattice* h, Path* out) {
                     "and stationary walls");
       path = Path::Lean;
       break;
+    case WT_KERNEL_PAIR:
+      if (!pair_ok(h))
+        return fail(h, WT_ERR_UNSUPPORTED,
+                    "the pair kernel needs half storage, the float32 collision, an even nx, "
+                    "buffers under 2 GiB and stationary walls");
+      path = Path::Pair;
+      break;
     case WT_KERNEL_AUTO:
       path = auto_path(h);
       break;
@@ -630,10 +653,12 @@ int select_path(wt_lattice* h, Path* out) {
 }
 
 template <class S>
-StepLaunch<S> pick(Path path, StepLaunch<S> direct, StepLaunch<S> lean, StepLaunch<S> pbb) {
+StepLaunch<S> pick(Path path, StepLaunch<S> direct, StepLaunch<S> lean, StepLaunch<S> pbb,
+                   StepLaunch<S> pair = nullptr) {
   switch (path) {
     case Path::Lean: return lean;
     case Path::Pbb: return pbb;
+    case Path::Pair: return pair ? pair : direct;
     default: return direct;
   }
 }
@@ -658,7 +683,7 @@ void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* part, double* 
     case WT_STORE_F16DEV:
       run_steps<__half>(h, nsteps,
                         pick<__half>(path, wt::launch_step_f16_fast, wt::launch_lean_f16,
-                                     wt::launch_pbb_f16_fast),
+                                     wt::launch_pbb_f16_fast, wt::launch_pair_f16),
                         part, forces_dev, err, chunk);
       break;
     default:

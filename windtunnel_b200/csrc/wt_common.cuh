@@ -134,6 +134,7 @@ struct StepArgs {
   int gx;              // x-segments (units) per row
   long long units;     // gx*ny*nz
   S eq[Q];             // equilibrium deviation at rho=1, u=(u0,0,0), rounded to S
+  uint32_t eq2[Q];     // half storage: eq[q] in both halves of a 32-bit word
   const double* sfrac; // partial bounce-back: solid fraction on the box sb (x fastest), or null
   int sb[6];           // its half-open box x0, y0, z0, x1, y1, z1
   long long pf;        // L2 prefetch distance in cells (0: none), see prefetch_ahead

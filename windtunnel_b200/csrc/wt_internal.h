@@ -88,6 +88,10 @@ void launch_adj_f64(const StepArgs<double>& a, const double* Tn, double* Tc, dou
 void launch_lean_f32(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
 void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
 
+// Half storage, two adjacent cells per thread with the packed float32x2
+// collision; the lean kernel's conditions and an even nx (grid is ignored).
+void launch_pair_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
+
 // Load the device code of every step and reduction kernel a wt_step call can
 // launch (cudaFuncGetAttributes on each), so that none is loaded lazily
 // inside a later call. The exact variant covers the --fmad=false unit.

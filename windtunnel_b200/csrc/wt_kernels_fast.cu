@@ -4,6 +4,7 @@
 #include "wt_internal.h"
 #include "wt_pbb.cuh"
 #include "wt_lean.cuh"
+#include "wt_pair.cuh"
 
 namespace wt {
 
@@ -23,6 +24,13 @@ void launch_lean_f32(const StepArgs<float>& a, dim3 grid, bool, cudaStream_t s) 
 
 void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool, cudaStream_t s) {
   k_step_lean<__half><<<grid, STEP_BX, 0, s>>>(a);
+}
+
+void launch_pair_f16(const StepArgs<__half>& a, dim3, bool, cudaStream_t s) {
+  const dim3 g((unsigned)((a.nx + 2 * PAIR_BX - 1) / (2 * PAIR_BX)), (unsigned)a.ny,
+               (unsigned)a.nz);
+  if (a.f16_sr) k_step_pair<true><<<g, PAIR_BX, 0, s>>>(a);
+  else k_step_pair<false><<<g, PAIR_BX, 0, s>>>(a);
 }
 
 // ---- partial bounce-back and adjoint (float32 arithmetic) -------------------------
@@ -111,6 +119,7 @@ cudaError_t preload_step_kernels() {
       (const void*)k_step<float, false, int>, (const void*)k_step<float, false, long long>,
       (const void*)k_step<__half, false, int>, (const void*)k_step<__half, false, long long>,
       (const void*)k_step_lean<float>, (const void*)k_step_lean<__half>,
+      (const void*)k_step_pair<false>, (const void*)k_step_pair<true>,
       (const void*)k_force_reduce};
   for (const void* f : fns) {
     const cudaError_t e = cudaFuncGetAttributes(&fa, f);

@@ -1,0 +1,414 @@
+// wt_pair.cuh — the fused step for half storage, two adjacent cells per
+// thread, both collided at once with sm_100's packed float32x2 instructions.
+//
+// Same semantics and per-cell rules as k_step (wt_step.cuh) and the lean
+// kernel: js/lbm.js:303-466 (stepSlab) followed by js/lbm.js:473-512
+// (_boundaries), the collision of collide_x2 (js/lbm.js:377-460
+// re-associated over opposite pairs) in the storage's scaled units.
+//
+// Thread t of block b owns cells x0 = 2 (b*PAIR_BX + t) and x0 + 1 of row
+// (y, z); nx is even, so every 32-bit word (x0, x0+1) of a population plane
+// is aligned. What the layout of the work buys, per pair of cells:
+//   * one 32-bit load per direction (the x-shifted directions add one 16-bit
+//     load of the neighbouring half at the same address +-2 bytes and a byte
+//     permute), one 32-bit store, one conversion to half pair;
+//   * every floating-point operation of the collision issued once for both
+//     cells (FADD2 / FMUL2 / FFMA2); only the five reciprocals / square roots
+//     per cell stay scalar.
+// Registers: the 19 loaded words stay packed as half pairs. A first pass
+// converts them pair of directions by pair and accumulates the moments
+// (density, momentum, the six second moments); the equilibrium and the
+// Smagorinsky stress follow from those analytically (the D3Q19 equilibrium's
+// second moment is dr/3 + r u u). A second pass converts the words again and
+// writes each output word as soon as it is formed.
+//
+// Boundary cells: the inlet cell x = 0 stores the equilibrium and the outlet
+// cell x = nx-1 stores a copy of cell nx-2 (js/lbm.js:504-511); both sit in
+// a pair whose other cell is computed, so the store of that pair selects its
+// halves with one byte permute per word (the outlet half takes the computed
+// half of cell nx-2, its own arithmetic is discarded). Near-wall and
+// free-slip shell cells re-gather the affected halves of their words before
+// the first pass; solid cells keep their stale populations (pairs holding
+// one store only the other half). Rows of the edge planes and the floor row
+// (whose cells are solid or equilibrium) take their own store-only paths.
+// Conditions: half storage, float32 collision, stationary walls, nx even,
+// both population buffers under 2^31 bytes (the lean kernel's 32-bit byte
+// offsets, StepArgs srcb / dstb).
+#pragma once
+
+#include "wt_x2.cuh"
+
+namespace wt {
+
+constexpr int PAIR_BX = 64;          // threads per block: 128 cells of one row
+constexpr int PAIR_MIN_BLOCKS = 8;  // 1024 resident threads per SM: 64 registers
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+  return __byte_perm(a, b, sel);
+}
+
+// half pair word (lo = cell x0, hi = cell x0+1) -> float pair (.x, .y)
+__device__ __forceinline__ f2 h2f(uint32_t w) {
+  __half2 h;
+  memcpy(&h, &w, 4);
+  return __half22float2(h);
+}
+
+// float pair -> half pair word, round to nearest
+__device__ __forceinline__ uint32_t f2h(f2 v) {
+  const __half2 h = __float22half2_rn(v);
+  uint32_t w;
+  memcpy(&w, &h, 4);
+  return w;
+}
+
+// float pair -> half pair word, stochastic rounding with 32 random bits
+__device__ __forceinline__ uint32_t f2h_sr(f2 v, uint32_t rbits) {
+  const __half2 h = sr_half2(v.y, v.x, rbits);   // (hi <- .y, lo <- .x)
+  uint32_t w;
+  memcpy(&w, &h, 4);
+  return w;
+}
+
+__device__ __forceinline__ uint32_t ld32(const char* p) {
+  return *reinterpret_cast<const uint32_t*>(p);
+}
+__device__ __forceinline__ uint32_t ld16(const char* p) {
+  return *reinterpret_cast<const uint16_t*>(p);
+}
+
+// Byte-permute selector that writes the half v (low 16 bits) into half L of w.
+__device__ __forceinline__ uint32_t put_half(uint32_t w, uint32_t v, int L) {
+  return prmt(w, v, L ? 0x5410u : 0x3254u);
+}
+
+// Re-gather the bounce-back and free-slip directions of cell xL = x0 + L (raw
+// half bits into half L of each word), js/lbm.js:334-368 for the bounce-back
+// links (stationary walls). The momentum exchange of body links accumulates
+// in float64 in raw units.
+__device__ __forceinline__ void pair_patch(const StepArgs<__half>& a, long long iL, int xL, int y,
+                                           int z, bool near_cell, bool shell, int L,
+                                           uint32_t (&w)[Q], double& Fx, double& Fy,
+                                           double& Fz) {
+  const unsigned long long m = near_cell ? a.nmask[iL] : 0ull;
+  const unsigned sm = (unsigned)m, om = (unsigned)(m >> 32);
+  const uint16_t* F = reinterpret_cast<const uint16_t*>(a.F);
+#define WT_PAIR_PATCH(q)                                                                   \
+  if ((sm >> (q)) & 1u) {                                                                  \
+    const uint32_t v = F[opp(q) * a.n + iL];                                               \
+    if ((om >> (q)) & 1u) {                                                                \
+      __half hv;                                                                           \
+      const uint16_t hb = (uint16_t)v;                                                     \
+      memcpy(&hv, &hb, 2);                                                                 \
+      const float d = 2.0f * __half2float(hv);                                             \
+      Fx -= (double)(d * (float)ex(q));                                                    \
+      Fy -= (double)(d * (float)ey(q));                                                    \
+      Fz -= (double)(d * (float)ez(q));                                                    \
+    }                                                                                      \
+    w[q] = put_half(w[q], v, L);                                                           \
+  } else if (shell) {                                                                      \
+    int sy = y - ey(q), sz = z - ez(q), qq = q;                                            \
+    bool refl = false;                                                                     \
+    if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); refl = true; }             \
+    if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); refl = true; }             \
+    if (refl)                                                                              \
+      w[q] = put_half(w[q], F[qq * a.n + (xL - ex(q)) + (long long)a.nx * sy + a.nxy * sz], \
+                      L);                                                                  \
+  }
+  WT_PAIR_PATCH(1) WT_PAIR_PATCH(2) WT_PAIR_PATCH(3) WT_PAIR_PATCH(4) WT_PAIR_PATCH(5)
+  WT_PAIR_PATCH(6) WT_PAIR_PATCH(7) WT_PAIR_PATCH(8) WT_PAIR_PATCH(9) WT_PAIR_PATCH(10)
+  WT_PAIR_PATCH(11) WT_PAIR_PATCH(12) WT_PAIR_PATCH(13) WT_PAIR_PATCH(14) WT_PAIR_PATCH(15)
+  WT_PAIR_PATCH(16) WT_PAIR_PATCH(17) WT_PAIR_PATCH(18)
+#undef WT_PAIR_PATCH
+}
+
+// Force partial of a pair-kernel warp: its 64 cells are two 32-cell
+// segments (lanes 0-15 and 16-31). Each half-warp that holds a near-wall
+// cell sums its doubles in a fixed order and its first lane stores them in
+// the segment's slot. Every lane must call it.
+__device__ __forceinline__ void pair_force_partial(double fx, double fy, double fz,
+                                                   bool near_cell, const StepArgs<__half>& a) {
+  const unsigned any = __ballot_sync(0xffffffffu, near_cell);
+  if (any == 0u) return;
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) {
+    fx += __shfl_down_sync(0xffffffffu, fx, o, 16);
+    fy += __shfl_down_sync(0xffffffffu, fy, o, 16);
+    fz += __shfl_down_sync(0xffffffffu, fz, o, 16);
+  }
+  const int lane = threadIdx.x & 31;
+  const unsigned half_bits = lane < 16 ? (any & 0xffffu) : (any >> 16);
+  if ((lane & 15) == 0 && half_bits) {
+    const int x = 2 * (blockIdx.x * PAIR_BX + (threadIdx.x & ~15));
+    const int slot = a.wslot[seg_of(x, blockIdx.y, blockIdx.z, a.nx, a.ny)];
+    if (slot >= 0) {
+      a.part[3 * (size_t)slot] = fx;
+      a.part[3 * (size_t)slot + 1] = fy;
+      a.part[3 * (size_t)slot + 2] = fz;
+    } else {
+      atomicOr(a.err, 2u);   // slot table out of date: reported, never silently dropped
+    }
+  }
+}
+
+template <bool SR>
+__global__ void __launch_bounds__(PAIR_BX, PAIR_MIN_BLOCKS)
+    k_step_pair(const __grid_constant__ StepArgs<__half> a) {
+  constexpr float SC = (float)WT_F16_SCALE;
+  const int x0 = 2 * (blockIdx.x * PAIR_BX + threadIdx.x);
+  const int y = blockIdx.y, z = blockIdx.z;
+  const long long i0 = (long long)x0 + (long long)a.nx * y + a.nxy * z;
+  double Fx = 0, Fy = 0, Fz = 0;
+  bool near_out = false;
+  if (x0 < a.nx) {
+    char* Gb = reinterpret_cast<char*>(a.G + i0);
+    auto gw = [&](int q) -> uint32_t& { return *reinterpret_cast<uint32_t*>(Gb + a.dstb[q]); };
+    auto gh = [&](int q, int L) -> uint16_t& {
+      return *reinterpret_cast<uint16_t*>(Gb + a.dstb[q] + 2 * L);
+    };
+    if (z == 0 || z == a.nz - 1 || y == a.ny - 1) {
+      // end planes and ceiling: the free-stream equilibrium (js/lbm.js:490-503)
+#pragma unroll
+      for (int q = 0; q < Q; q++) gw(q) = a.eq2[q];
+      if (a.write_fields) {
+        *reinterpret_cast<float2*>(a.ux + i0) = make_float2(a.u0f, a.u0f);
+        *reinterpret_cast<float2*>(a.uy + i0) = make_float2(0.f, 0.f);
+        *reinterpret_cast<float2*>(a.uz + i0) = make_float2(0.f, 0.f);
+        *reinterpret_cast<float2*>(a.rho + i0) = make_float2(1.f, 1.f);
+      }
+    } else if (y == 0) {
+      // floor row: equilibrium unless solid (js/lbm.js:492-494), the inlet
+      // cell always (js/lbm.js:489 comes first); the outlet copies column
+      // nx-2, which ends up as that column's choice
+      const uint32_t fl = ld16(reinterpret_cast<const char*>(a.flags + i0));
+      const bool outlet = x0 == a.nx - 2;
+#pragma unroll
+      for (int L = 0; L < 2; L++) {
+        const uint32_t fb = (L == 0 && x0 == 0) ? 0u : (outlet ? fl : (fl >> (8 * L)));
+        if (fb & FLAG_SOLID_MASK) {
+          if (L == 1 && outlet) {
+#pragma unroll
+            for (int q = 0; q < Q; q++) gh(q, 1) = gh(q, 0);
+            if (a.write_fields) {
+              a.ux[i0 + 1] = a.ux[i0]; a.uy[i0 + 1] = a.uy[i0];
+              a.uz[i0 + 1] = a.uz[i0]; a.rho[i0 + 1] = a.rho[i0];
+            }
+          }
+          continue;
+        }
+#pragma unroll
+        for (int q = 0; q < Q; q++) gh(q, L) = (uint16_t)a.eq2[q];
+        if (a.write_fields) {
+          a.ux[i0 + L] = a.u0f; a.uy[i0 + L] = 0.f; a.uz[i0 + L] = 0.f; a.rho[i0 + L] = 1.f;
+        }
+      }
+    } else {
+      // interior row: pull every direction of both cells. The sources of
+      // the pair (x0 - ex, x0 + 1 - ex) of row (y - ey, z - ez) lie inside
+      // the buffer for every cell of an interior row.
+      const char* Fb = reinterpret_cast<const char*>(a.F + i0);
+      uint32_t w[Q];
+#define WT_PAIR_LOAD(q)                                                                  \
+  {                                                                                      \
+    const char* p = Fb + a.srcb[q];   /* byte address of the source of cell x0 */        \
+    if constexpr (ex(q) == 0) {                                                          \
+      w[q] = ld32(p);                                                                    \
+    } else if constexpr (ex(q) == 1) {                                                   \
+      /* (x0-1, x0): the half at p, then the low half of the word at p+2 */              \
+      w[q] = prmt(ld16(p), ld32(p + 2), 0x5410u);                                        \
+    } else {                                                                             \
+      /* (x0+1, x0+2): the high half of the word at p-2, then the half at p+2 */         \
+      w[q] = prmt(ld32(p - 2), ld16(p + 2), 0x5432u);                                    \
+    }                                                                                    \
+  }
+      WT_PAIR_LOAD(0) WT_PAIR_LOAD(1) WT_PAIR_LOAD(2) WT_PAIR_LOAD(3) WT_PAIR_LOAD(4)
+      WT_PAIR_LOAD(5) WT_PAIR_LOAD(6) WT_PAIR_LOAD(7) WT_PAIR_LOAD(8) WT_PAIR_LOAD(9)
+      WT_PAIR_LOAD(10) WT_PAIR_LOAD(11) WT_PAIR_LOAD(12) WT_PAIR_LOAD(13) WT_PAIR_LOAD(14)
+      WT_PAIR_LOAD(15) WT_PAIR_LOAD(16) WT_PAIR_LOAD(17) WT_PAIR_LOAD(18)
+#undef WT_PAIR_LOAD
+      const uint32_t fl = ld16(reinterpret_cast<const char*>(a.flags + i0));
+      const bool inlet = x0 == 0;
+      const bool outlet = x0 == a.nx - 2;
+      const bool solid0 = (fl & FLAG_SOLID_MASK) != 0;
+      // the outlet cell is a copy of cell nx-2 whatever its own code
+      const bool solid1 = !outlet && ((fl >> 8) & FLAG_SOLID_MASK) != 0;
+      // cells whose collision is kept: cell 0 unless inlet or solid; cell 1
+      // unless solid or the outlet copy
+      const bool fluid0 = !inlet && !solid0;
+      const bool fluid1 = !outlet && !solid1;
+      const bool near0 = fluid0 && (fl & FLAG_NEAR);
+      const bool near1 = fluid1 && ((fl >> 8) & FLAG_NEAR);
+      const bool shell = a.freeslip && (y == 1 || y == a.ny - 2 || z == 1 || z == a.nz - 2);
+      if (near0 || (shell && fluid0))
+        pair_patch(a, i0, x0, y, z, near0, shell, 0, w, Fx, Fy, Fz);
+      if (near1 || (shell && fluid1))
+        pair_patch(a, i0 + 1, x0 + 1, y, z, near1, shell, 1, w, Fx, Fy, Fz);
+      near_out = near0 || near1;
+
+      // ---- pass 1: moments --------------------------------------------------
+      f2 dr, jx, jy, jz, pxx, pyy, pzz, pxy, pxz, pyz;
+      {
+        const f2 f0 = h2f(w[0]);
+        f2 fa = h2f(w[1]), fb = h2f(w[2]);
+        f2 s = padd(fa, fb), d = psub(fa, fb);
+        dr = padd(f0, s); jx = d; pxx = s;
+        fa = h2f(w[3]); fb = h2f(w[4]); s = padd(fa, fb); d = psub(fa, fb);
+        dr = padd(dr, s); jy = d; pyy = s;
+        fa = h2f(w[5]); fb = h2f(w[6]); s = padd(fa, fb); d = psub(fa, fb);
+        dr = padd(dr, s); jz = d; pzz = s;
+        fa = h2f(w[7]); fb = h2f(w[8]); s = padd(fa, fb); d = psub(fa, fb);
+        dr = padd(dr, s); jx = padd(jx, d); jy = padd(jy, d); pxx = padd(pxx, s);
+        pyy = padd(pyy, s); pxy = s;
+        fa = h2f(w[9]); fb = h2f(w[10]); s = padd(fa, fb); d = psub(fa, fb);
+        dr = padd(dr, s); jx = padd(jx, d); jy = psub(jy, d); pxx = padd(pxx, s);
+        pyy = padd(pyy, s); pxy = psub(pxy, s);
+        fa = h2f(w[11]); fb = h2f(w[12]); s = padd(fa, fb); d = psub(fa, fb);
+        dr = padd(dr, s); jx = padd(jx, d); jz = padd(jz, d); pxx = padd(pxx, s);
+        pzz = padd(pzz, s); pxz = s;
+        fa = h2f(w[13]); fb = h2f(w[14]); s = padd(fa, fb); d = psub(fa, fb);
+        dr = padd(dr, s); jx = padd(jx, d); jz = psub(jz, d); pxx = padd(pxx, s);
+        pzz = padd(pzz, s); pxz = psub(pxz, s);
+        fa = h2f(w[15]); fb = h2f(w[16]); s = padd(fa, fb); d = psub(fa, fb);
+        dr = padd(dr, s); jy = padd(jy, d); jz = padd(jz, d); pyy = padd(pyy, s);
+        pzz = padd(pzz, s); pyz = s;
+        fa = h2f(w[17]); fb = h2f(w[18]); s = padd(fa, fb); d = psub(fa, fb);
+        dr = padd(dr, s); jy = padd(jy, d); jz = psub(jz, d); pyy = padd(pyy, s);
+        pzz = padd(pzz, s); pyz = psub(pyz, s);
+      }
+      // ---- macroscopic state, relaxation rates -------------------------------
+      const f2 r = padd(pk(SC), dr);
+      const f2 inv = prcp(r);
+      const f2 vx = pmul(jx, inv), vy = pmul(jy, inv), vz = pmul(jz, inv);
+      const f2 usq = pfma(vz, vz, pfma(vy, vy, pmul(vx, vx)));
+      const f2 A = pfma(pmul(pk(-1.5f), r), usq, dr);   // dr - 1.5 r u^2 (raw)
+      const bool ok0 = !fluid0 || (r.x > 0.0f && r.x < 3.0e38f);
+      const bool ok1 = !fluid1 || (r.y > 0.0f && r.y < 3.0e38f);
+      if (!(ok0 && ok1)) atomicOr(a.err, 1u);
+      f2 om = pk(a.omega0f), omm = pk(a.omm0f);
+      if (a.les) {
+        // non-equilibrium second moments: P - (dr/3 + r u u), js/lbm.js:420-425
+        const f2 rvx = pmul(r, vx), rvy = pmul(r, vy), rvz = pmul(r, vz);
+        const f2 dr3 = pmul(pk(1.0f / 3.0f), dr);
+        const f2 sxx = pfma(pmul(pk(-1.0f), rvx), vx, psub(pxx, dr3));
+        const f2 syy = pfma(pmul(pk(-1.0f), rvy), vy, psub(pyy, dr3));
+        const f2 szz = pfma(pmul(pk(-1.0f), rvz), vz, psub(pzz, dr3));
+        const f2 sxy = pfma(pmul(pk(-1.0f), rvx), vy, pxy);
+        const f2 sxz = pfma(pmul(pk(-1.0f), rvx), vz, pxz);
+        const f2 syz = pfma(pmul(pk(-1.0f), rvy), vz, pyz);
+        const f2 off = pfma(syz, syz, pfma(sxz, sxz, pmul(sxy, sxy)));
+        const f2 q2 = pfma(sxx, sxx, pfma(syy, syy, pfma(szz, szz, padd(off, off))));
+        // 18 sqrt(2) Cs^2 |Pi| / rho with |Pi| = sqrt(2 q2): 36 Cs^2 sqrt(q2) / r
+        const f2 x = pmul(pmul(pk(0.5f * a.les_cf), psqrt(q2)), inv);
+        const f2 te = pfma(pk(0.5f), psqrt(pfma(pk(a.tau0f), pk(a.tau0f), x)), pk(0.5f * a.tau0f));
+        om = prcp(te);
+        if (a.trt) {
+          const f2 t5 = psub(te, pk(0.5f));
+          omm = pmul(t5, prcp(pfma(pk(0.5f), t5, pk(a.lamf))));
+        } else {
+          omm = om;
+        }
+      }
+      if (a.write_fields) {
+        const f2 rho = pmul(r, pk(1.0f / SC));
+        if (fluid0 && (fluid1 || outlet)) {
+          const float2 u = outlet ? make_float2(vx.x, vx.x) : vx;
+          const float2 v = outlet ? make_float2(vy.x, vy.x) : vy;
+          const float2 ww = outlet ? make_float2(vz.x, vz.x) : vz;
+          const float2 rr = outlet ? make_float2(rho.x, rho.x) : rho;
+          *reinterpret_cast<float2*>(a.ux + i0) = u;
+          *reinterpret_cast<float2*>(a.uy + i0) = v;
+          *reinterpret_cast<float2*>(a.uz + i0) = ww;
+          *reinterpret_cast<float2*>(a.rho + i0) = rr;
+        } else {
+          if (fluid0) {
+            a.ux[i0] = vx.x; a.uy[i0] = vy.x; a.uz[i0] = vz.x; a.rho[i0] = rho.x;
+          } else if (inlet) {
+            a.ux[i0] = a.u0f; a.uy[i0] = 0.f; a.uz[i0] = 0.f; a.rho[i0] = 1.f;
+          }
+          if (fluid1) {
+            a.ux[i0 + 1] = vx.y; a.uy[i0 + 1] = vy.y; a.uz[i0 + 1] = vz.y;
+            a.rho[i0 + 1] = rho.y;
+          } else if (outlet) {
+            // copy of a solid cell nx-2: its fields as they stand
+            a.ux[i0 + 1] = a.ux[i0]; a.uy[i0 + 1] = a.uy[i0];
+            a.uz[i0 + 1] = a.uz[i0]; a.rho[i0 + 1] = a.rho[i0];
+          }
+        }
+      }
+      // ---- per-cell constants of the update ---------------------------------
+      // g_a = P + M, g_b = P - M over the opposite pair (a, b) with
+      //   P = (1 - om)/2 s + om w (A + 4.5 r c^2),  M = (1 - omm)/2 d + omm 3 w r c
+      // (s = f_a + f_b, d = f_a - f_b, c = c_a . u); w = 1/18 face, 1/36 edge
+      const f2 al = pfma(pk(-0.5f), om, pk(0.5f));
+      const f2 be = pfma(pk(-0.5f), omm, pk(0.5f));
+      const f2 omr = pmul(om, r), ommr = pmul(omm, r), omA = pmul(om, A);
+      const f2 k45f = pmul(pk(0.25f), omr), k45e = pmul(pk(0.125f), omr);
+      const f2 kaf = pmul(pk((float)(1.0 / 18)), omA), kae = pmul(pk((float)(1.0 / 36)), omA);
+      const f2 k3f = pmul(pk((float)(1.0 / 6)), ommr), k3e = pmul(pk((float)(1.0 / 12)), ommr);
+      // store selection: the inlet's low half takes the equilibrium, the
+      // outlet's high half takes cell nx-2's half
+      const uint32_t sel = inlet ? 0x3254u : (outlet ? 0x1010u : 0x3210u);
+      // a solid cell keeps its stale populations, and so does the outlet copy
+      // of a solid cell nx-2 until the copy below
+      const bool keep0 = solid0 && !inlet, keep1 = solid1 || (outlet && solid0);
+      const bool keep_any = keep0 || keep1;
+      uint32_t h = 0;
+      if constexpr (SR) {
+        h = ((uint32_t)i0 ^ (uint32_t)(i0 >> 32)) * 0x9E3779B1u ^ a.sr_seed;
+        h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+      }
+      auto put = [&](int q, f2 g) {
+        uint32_t v;
+        if constexpr (SR) {
+          h ^= h << 13; h ^= h >> 17; h ^= h << 5;
+          v = f2h_sr(g, h);
+        } else {
+          v = f2h(g);
+        }
+        v = prmt(v, a.eq2[q], sel);
+        if (!keep_any) {
+          gw(q) = v;
+        } else {
+          // a solid cell of the pair keeps its stale population
+          if (!keep0) gh(q, 0) = (uint16_t)v;
+          if (!keep1) gh(q, 1) = (uint16_t)(v >> 16);
+        }
+      };
+      // ---- pass 2: outputs ----------------------------------------------------
+      {
+        const f2 f0 = h2f(w[0]);
+        put(0, pfma(pfma(pk(-1.0f), om, pk(1.0f)), f0, pmul(pk((float)(1.0 / 3)), omA)));
+      }
+#define WT_PAIR_OUT(qa, C, K45, KA, K3)                 \
+  {                                                     \
+    const f2 fa = h2f(w[qa]), fb = h2f(w[qa + 1]);      \
+    const f2 s = padd(fa, fb), d = psub(fa, fb);        \
+    const f2 c = C;                                     \
+    const f2 X = pfma(pmul(c, c), K45, KA);             \
+    const f2 Y = pmul(K3, c);                           \
+    const f2 P = pfma(al, s, X), M = pfma(be, d, Y);    \
+    put(qa, padd(P, M));                                \
+    put(qa + 1, psub(P, M));                            \
+  }
+      WT_PAIR_OUT(1, vx, k45f, kaf, k3f)
+      WT_PAIR_OUT(3, vy, k45f, kaf, k3f)
+      WT_PAIR_OUT(5, vz, k45f, kaf, k3f)
+      WT_PAIR_OUT(7, padd(vx, vy), k45e, kae, k3e)
+      WT_PAIR_OUT(9, psub(vx, vy), k45e, kae, k3e)
+      WT_PAIR_OUT(11, padd(vx, vz), k45e, kae, k3e)
+      WT_PAIR_OUT(13, psub(vx, vz), k45e, kae, k3e)
+      WT_PAIR_OUT(15, padd(vy, vz), k45e, kae, k3e)
+      WT_PAIR_OUT(17, psub(vy, vz), k45e, kae, k3e)
+#undef WT_PAIR_OUT
+      if (outlet && solid0) {
+        // copy of a solid cell nx-2, whose g this step does not write
+#pragma unroll
+        for (int q = 0; q < Q; q++) gh(q, 1) = gh(q, 0);
+      }
+    }
+  }
+  constexpr double inv_sc = 1.0 / (double)SC;   // a power of two: exact
+  pair_force_partial(Fx * inv_sc, Fy * inv_sc, Fz * inv_sc, near_out, a);
+}
+
+}  // namespace wt

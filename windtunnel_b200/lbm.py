@@ -31,7 +31,8 @@ FLUID, SOLID_OBJ, SOLID_WALL = W.WT_FLUID, W.WT_SOLID_OBJ, W.WT_SOLID_WALL
 STORAGE = {"f32": W.WT_STORE_F32, "f16dev": W.WT_STORE_F16DEV, "f64": W.WT_STORE_F64}
 MATH = {"fast": W.WT_MATH_FAST, "exact": W.WT_MATH_EXACT}
 SIDE = {"eq": W.WT_SIDE_EQ, "freeslip": W.WT_SIDE_FREESLIP}
-KERNEL = {"auto": W.WT_KERNEL_AUTO, "direct": W.WT_KERNEL_DIRECT, "lean": W.WT_KERNEL_LEAN}
+KERNEL = {"auto": W.WT_KERNEL_AUTO, "direct": W.WT_KERNEL_DIRECT, "lean": W.WT_KERNEL_LEAN,
+          "pair": W.WT_KERNEL_PAIR}
 _STORE_DTYPE = {W.WT_STORE_F32: np.float32, W.WT_STORE_F16DEV: np.float16,
                 W.WT_STORE_F64: np.float64}
 
