@@ -300,53 +300,89 @@ def pair_avg_coeff(forces, u0, area, window):
     return float(w[:, 0].mean() / q), float(w[:, 1].mean() / q)
 
 
-def accuracy_study(wl, long_steps: int = 20000) -> dict:
-    """Cd / Cl of every storage form vs FP64, with blocking standard errors.
+ACCURACY_FORMS = (("f64", "f64", "exact", None), ("f32", "f32", "fast", None),
+                  ("f16dev", "f16dev", "fast", "nearest"),
+                  ("f16dev_stochastic", "f16dev", "fast", "stochastic"))
 
-    Each form runs the workload's step count and reports the pair-averaged
-    coefficients over its last `window` steps (the configuration's
-    statistic), then runs `long_steps` more and reports the average over
-    those as well, which separates a bias of the storage form from the
-    sampling noise of a turbulent wake.
-    """
+
+def accuracy_study(wl, replicas: int = 4, steps: int | None = None,
+                   window: int | None = None) -> dict:
+    """Cd / Cl of every storage form against float64 storage, as ensemble means.
+
+    The hull's wake at Re 2000 is chaotic: two arithmetic forms (float32
+    included) follow different trajectories after a few thousand steps, so
+    one run's window average carries a sampling error of several percent of
+    Cd. Each form therefore runs `replicas` seeded copies of the workload
+    (initial velocity noise seeds seed, seed+1, ...; the same seeds for every
+    form) for the configuration's step count and takes the pair-averaged
+    coefficients over the last `window` steps of each (js/main.js:113-127).
+    A form's Cd is the mean over its replicas with the standard error
+    std / sqrt(replicas); its error against float64 (and float32) is the mean
+    of the per-seed differences, with their standard error."""
+    import numpy as np
+
     from windtunnel_b200.stats import window_coefficients
-    out = {"steps": wl["accuracy_steps"], "window": wl["accuracy_window"],
-           "long_window": long_steps,
-           "average": "pair-averaged consecutive steps (js/main.js:113-127), "
-                      "16-block blocking SEM (js/main.js:163-191)"}
-    res = {}
-    forms = (("f64", "f64", "exact", None), ("f32", "f32", "fast", None),
-             ("f16dev", "f16dev", "fast", "nearest"),
-             ("f16dev_stochastic", "f16dev", "fast", "stochastic"))
-    for name, storage, mm, rounding in forms:
+    steps = steps or wl["accuracy_steps"]
+    window = window or wl["accuracy_window"]
+    out = {"workload": wl["name"], "steps": steps, "window": window, "replicas": replicas,
+           "seeds": [wl["seed"] + k for k in range(replicas)],
+           "statistic": "mean over seeded replicas of the pair-averaged coefficient over "
+                        "the last `window` steps; sem = std / sqrt(replicas)"}
+    per = {}
+    for name, storage, mm, rounding in ACCURACY_FORMS:
         sim = setup_gpu(wl, storage, mm)
         if rounding:
             sim.set_params(f16_rounding=rounding)
+        cd, cl = [], []
         t0 = time.time()
-        F = sim.step_forces(wl["accuracy_steps"])
-        short = window_coefficients(F, wl["u0"], sim.frontalArea, wl["accuracy_window"])
-        F2 = sim.step_forces(long_steps) if long_steps else None
-        entry = {"cd": short["cd"], "cd_sem": short["cd_sem"], "cl": short["cl"],
-                 "cl_sem": short["cl_sem"]}
-        if F2 is not None:
-            lw = window_coefficients(F2, wl["u0"], sim.frontalArea, long_steps - 1)
-            entry.update(cd_long=lw["cd"], cd_long_sem=lw["cd_sem"], cl_long=lw["cl"],
-                         cl_long_sem=lw["cl_sem"])
-        entry["wall_s"] = round(time.time() - t0, 2)
-        if rounding:
-            entry["rounding"] = rounding
-        res[name] = entry
+        for k in range(replicas):
+            sim.init_eq_noise(wl["seed"] + k, wl["amp"])
+            F = sim.step_forces(steps)
+            c = window_coefficients(F, wl["u0"], sim.frontalArea, window)
+            cd.append(c["cd"])
+            cl.append(c["cl"])
         sim.close()
-    ref = res["f64"]
-    for name, e in res.items():
-        if name == "f64":
-            continue
-        e["dcd_rel_vs_f64"] = abs(e["cd"] - ref["cd"]) / abs(ref["cd"])
-        if "cd_long" in e:
-            e["dcd_long_rel_vs_f64"] = abs(e["cd_long"] - ref["cd_long"]) / abs(ref["cd_long"])
-            e["dcd_long_sigma"] = abs(e["cd_long"] - ref["cd_long"]) / math.hypot(
-                e["cd_long_sem"], ref["cd_long_sem"])
-    out.update(res)
+        per[name] = (np.array(cd), np.array(cl))
+        e = {"cd": float(np.mean(cd)), "cl": float(np.mean(cl)),
+             "cd_sem": float(np.std(cd, ddof=1) / math.sqrt(replicas)) if replicas > 1 else None,
+             "cl_sem": float(np.std(cl, ddof=1) / math.sqrt(replicas)) if replicas > 1 else None,
+             "cd_replicas": [round(v, 6) for v in cd], "wall_s": round(time.time() - t0, 2)}
+        if rounding:
+            e["rounding"] = rounding
+        out[name] = e
+    for ref in ("f64", "f32"):
+        rcd, rcl = per[ref]
+        for name, (cd, cl) in per.items():
+            if name == ref or (ref == "f32" and name == "f64"):
+                continue
+            dcd, dcl = cd - rcd, cl - rcl
+            sem = float(np.std(dcd, ddof=1) / math.sqrt(replicas)) if replicas > 1 else None
+            out[name][f"dcd_rel_vs_{ref}"] = float(np.mean(dcd) / np.mean(rcd))
+            out[name][f"dcd_rel_vs_{ref}_sem"] = sem / abs(float(np.mean(rcd))) if sem else None
+            out[name][f"dcl_vs_{ref}_over_cd"] = float(np.mean(dcl) / np.mean(rcd))
+    return out
+
+
+def steady_accuracy(wl) -> dict:
+    """The storage error alone, on a steady wake: one run per form, Cd / Cl
+    over the last window steps against float64 storage."""
+    from windtunnel_b200.stats import window_coefficients
+    out = {"workload": wl["name"], "steps": wl["accuracy_steps"],
+           "window": wl["accuracy_window"]}
+    ref = None
+    for name, storage, mm, rounding in ACCURACY_FORMS:
+        sim = setup_gpu(wl, storage, mm)
+        if rounding:
+            sim.set_params(f16_rounding=rounding)
+        c = window_coefficients(sim.step_forces(wl["accuracy_steps"]), wl["u0"], sim.frontalArea,
+                                wl["accuracy_window"])
+        sim.close()
+        e = {"cd": c["cd"], "cl": c["cl"]}
+        if ref is None:
+            ref = e
+        else:
+            e["dcd_rel_vs_f64"] = abs(e["cd"] - ref["cd"]) / abs(ref["cd"])
+        out[name] = e
     return out
 
 
@@ -381,13 +417,13 @@ def design_field(aw) -> "np.ndarray":
     return np.clip(s, 0.0, 1.0)
 
 
-def design_lattice(aw, storage, math_mode="fast", s=None):
+def design_lattice(aw, storage, math_mode="fast", s=None, seed=None):
     from windtunnel_b200 import LBM
     sim = LBM(aw["nx"], aw["ny"], aw["nz"], storage=storage, math=math_mode,
               side_bc=aw["side_bc"])
     sim.set_params(u0=aw["u0"], tau=aw["tau"], csm=aw["csm"], les=int(aw["les"]),
                    **{"lambda": aw["lam"]})
-    sim.init_eq_noise(aw["seed"], aw["amp"])
+    sim.init_eq_noise(aw["seed"] if seed is None else seed, aw["amp"])
     sim.set_solid_fraction(aw["box"], design_field(aw) if s is None else s)
     return sim
 
@@ -520,6 +556,37 @@ def adjoint_study(aw) -> dict:
         # Cd is J over the same dynamic pressure and area: the relative errors coincide
         out["cd_rel_err_vs_f64"] = abs(J_fwd - J64) / abs(J64)
     return out
+
+
+def adjoint_horizon_study(aw, horizons=(250, 500, 1000, 2000, 4000), window=250) -> dict:
+    """How far the half-storage and float32-storage gradients of one design
+    workload agree, against the horizon N (J = mean drag over the last
+    `window` steps of N): cosine and relative L2 of dJ/ds, and the relative
+    difference of J. Beside it, the same comparison between two float32
+    runs whose initial velocity noise differs (seed and seed + 1): the
+    agreement two trajectories of one arithmetic keep once the flow has
+    separated them, which the half/float32 pair cannot beat."""
+    import numpy as np
+
+    def grad(storage, N, seed=None):
+        sim = design_lattice(aw, storage, seed=seed)
+        J, g, _ = sim.adjoint(N, window, 0, 0)
+        sim.close()
+        return J, g
+
+    def agree(a, b):
+        (Ja, ga), (Jb, gb) = a, b
+        return {"cosine": float((ga * gb).sum() / (np.linalg.norm(ga) * np.linalg.norm(gb))),
+                "rel_l2": float(np.linalg.norm(ga - gb) / np.linalg.norm(gb)),
+                "J_rel": abs(Ja - Jb) / abs(Jb)}
+
+    rows = []
+    for N in horizons:
+        f32 = grad("f32", N)
+        rows.append({"steps": N, "half_vs_f32": agree(grad("f16dev", N), f32),
+                     "f32_reseeded_vs_f32": agree(grad("f32", N, aw["seed"] + 1), f32)})
+    return {"workload": aw["name"], "window": window,
+            "objective": "mean drag over the last window steps", "horizons": rows}
 
 
 def cpu_baseline(wl, budget_s: float = 24.0) -> dict:
@@ -688,8 +755,8 @@ def run_wt(args) -> None:
         "clocks": clk,
     }
     if args.accuracy and dist.rank == 0:
-        line["accuracy"] = accuracy_study(wl)
-        line["accuracy_steady"] = accuracy_study(WORKLOADS["sphere128"], long_steps=0)
+        line["accuracy"] = accuracy_study(wl, replicas=args.replicas)
+        line["accuracy_steady"] = steady_accuracy(WORKLOADS["sphere128"])
     if args.adjoint and dist.rank == 0:
         line["adjoint"] = adjoint_study(ADJOINT_WORKLOADS["design128"])
         if args.adjoint_scale:
@@ -749,6 +816,19 @@ def run_reference(args) -> None:
         flush=True)
 
 
+def run_study(args) -> None:
+    """`--study accuracy`: the accuracy ensemble on --workload with --replicas
+    seeds per form; `--study adjoint-horizon`: the half-vs-float32 gradient
+    agreement of the 384x160x160 differentiation workload against horizon."""
+    import torch
+    torch.cuda.set_device(0)
+    if args.study == "accuracy":
+        res = accuracy_study(WORKLOADS[args.workload], replicas=args.replicas)
+    else:
+        res = adjoint_horizon_study(ADJOINT_WORKLOADS["design384"])
+    print(json.dumps(res), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -757,6 +837,10 @@ def main() -> None:
     ap.add_argument("--impl", choices=["wt", "reference"], default="wt")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="channel256")
     ap.add_argument("--no-accuracy", dest="accuracy", action="store_false")
+    ap.add_argument("--replicas", type=int, default=4,
+                    help="seeded replicas per storage form in the accuracy ensemble")
+    ap.add_argument("--study", choices=["accuracy", "adjoint-horizon"],
+                    help="run one study alone and print its JSON (no timing line)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
     ap.add_argument("--no-adjoint-scale", dest="adjoint_scale", action="store_false")
@@ -767,6 +851,8 @@ def main() -> None:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.study:
+        run_study(args)
     else:
         run_wt(args)
 

@@ -41,7 +41,7 @@
 namespace wt {
 
 constexpr int PAIR_BX = 64;          // threads per block: 128 cells of one row
-constexpr int PAIR_MIN_BLOCKS = 8;  // 1024 resident threads per SM: 64 registers
+constexpr int PAIR_MIN_BLOCKS = 10;  // 640 resident threads per SM: 96 registers, no spills
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
   return __byte_perm(a, b, sel);
