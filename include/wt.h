@@ -85,9 +85,10 @@ enum {
                             distance ahead in launch order (environment WT_PREFETCH_CELLS
                             overrides the distance at wt_create, for any lattice; 0 turns it
                             off); float32 collision, buffers under 2 GiB, stationary walls */
-  WT_KERNEL_PAIR = 8     /* half storage: two adjacent cells per thread, one 32-bit load and
-                            store per direction and pair, both cells collided at once in
-                            packed float32x2 instructions; LEAN's conditions and an even nx */
+  WT_KERNEL_PAIR = 8     /* two adjacent cells per thread, one aligned load and store of the
+                            pair per direction (32-bit half pairs, 64-bit float32 pairs), both
+                            cells collided at once in packed float32x2 instructions; LEAN's
+                            conditions (half or float32 storage) and an even nx */
 };
 
 /* Rounding of half-precision stores. Stochastic rounding draws its random

@@ -75,6 +75,7 @@ void free_all(wt_lattice* h) {
   if (h->forces_host) cudaFreeHost(h->forces_host);
   if (h->err_host) cudaFreeHost(h->err_host);
   if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->aux) cudaStreamDestroy(h->aux);
   if (h->adj_pool) cudaFree(h->adj_pool);
   h->adj_pool = nullptr;
 }
@@ -215,7 +216,7 @@ bool pair_ok(const wt_lattice* h);
 // 44.3k against 37.2k), the direct kernel otherwise (exact collision,
 // float64, moving walls, buffers of 2^31 bytes or more).
 Path auto_path(const wt_lattice* h) {
-  if (pair_ok(h)) return Path::Pair;
+  if (h->storage == WT_STORE_F16DEV && pair_ok(h)) return Path::Pair;
   if (lean_ok(h)) return Path::Lean;
   return Path::Direct;
 }
@@ -229,11 +230,10 @@ bool lean_ok(const wt_lattice* h) {
   return !exact && !h->p.moving_walls && 19 * h->n * (long long)h->elem < (1LL << 31);
 }
 
-// True when the half-pair kernel can run: half storage, the lean kernel's
-// conditions and an even nx (aligned 32-bit pairs of cells).
-bool pair_ok(const wt_lattice* h) {
-  return h->storage == WT_STORE_F16DEV && lean_ok(h) && h->nx % 2 == 0;
-}
+// True when the pair kernel can run: the lean kernel's conditions (float32
+// collision, so half or float32 storage) and an even nx (aligned pairs of
+// cells).
+bool pair_ok(const wt_lattice* h) { return lean_ok(h) && h->nx % 2 == 0; }
 
 int select_path(wt_lattice* h, Path* out);
 void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* part, double* forces_dev,
@@ -638,8 +638,8 @@ int select_path(wt_lattice* h, Path* out) {
     case WT_KERNEL_PAIR:
       if (!pair_ok(h))
         return fail(h, WT_ERR_UNSUPPORTED,
-                    "the pair kernel needs half storage, the float32 collision, an even nx, "
-                    "buffers under 2 GiB and stationary walls");
+                    "the pair kernel needs the float32 collision, an even nx, buffers "
+                    "under 2 GiB and stationary walls");
       path = Path::Pair;
       break;
     case WT_KERNEL_AUTO:
@@ -677,7 +677,7 @@ void dispatch_steps(wt_lattice* h, int nsteps, Path path, double* part, double* 
       else
         run_steps<float>(h, nsteps,
                          pick<float>(path, wt::launch_step_f32_fast, wt::launch_lean_f32,
-                                     wt::launch_pbb_f32_fast),
+                                     wt::launch_pbb_f32_fast, wt::launch_pair_f32),
                          part, forces_dev, err, chunk);
       break;
     case WT_STORE_F16DEV:
@@ -1023,52 +1023,83 @@ int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_ad
   const size_t nbox = (size_t)(b[3] - b[0]) * (b[4] - b[1]) * (b[5] - b[2]);
   AdjBlock mem{h, cfg.keep != 0};
   const size_t pel = pop / sizeof(S);                // elements of one state
-  // checkpoints S^{kC} of every segment but the last, whose states the
-  // forward sweep writes straight into the segment store (C + 1 states)
+  // checkpoints S^{kC} of every interval but the last, whose states the
+  // forward sweep writes straight into an interval store (C + 1 states).
+  // With two stores the recomputation of interval k-1 runs on a second
+  // stream while the adjoint steps of interval k run on the lattice's
+  // stream; one store (when two do not fit) runs them in turn.
   const size_t sz_cps = ncp > 1 ? pop * (size_t)(ncp - 1) : 0, sz_seg = pop * (size_t)(C + 1);
   const size_t sz_ds = sizeof(double) * nbox, sz_f = sizeof(double) * 3 * (size_t)N;
-  const size_t total = AdjBlock::up(sz_cps) + AdjBlock::up(sz_seg) + 2 * AdjBlock::up(tsz) +
-                       AdjBlock::up(sz_ds) + AdjBlock::up(sz_f);
-  if (!mem.acquire(total))
+  auto total_for = [&](int stores) {
+    return AdjBlock::up(sz_cps) + stores * AdjBlock::up(sz_seg) + 2 * AdjBlock::up(tsz) +
+           AdjBlock::up(sz_ds) + AdjBlock::up(sz_f);
+  };
+  int ns = ncp > 1 ? 2 : 1;
+  size_t total = total_for(ns);
+  if (!mem.acquire(total) && ns == 2) {
+    cudaGetLastError();
+    ns = 1;
+    total = total_for(ns);
+    if (!mem.acquire(total))
+      return fail(h, WT_ERR_OOM, "cannot allocate the adjoint's checkpoints (" +
+                                     std::to_string(total >> 20) + " MiB)");
+  } else if (!mem.base) {
     return fail(h, WT_ERR_OOM, "cannot allocate the adjoint's checkpoints (" +
                                    std::to_string(total >> 20) + " MiB)");
+  }
+  cudaGetLastError();
   S* cps = ncp > 1 ? (S*)mem.carve(sz_cps) : nullptr;
-  S* seg = (S*)mem.carve(sz_seg);
+  S* seg[2] = {(S*)mem.carve(sz_seg), ns == 2 ? (S*)mem.carve(sz_seg) : nullptr};
+  if (ns == 1) seg[1] = seg[0];
   T* Tbuf[2] = {(T*)mem.carve(tsz), (T*)mem.carve(tsz)};
   double* ds = (double*)mem.carve(sz_ds);
   double* fdev = (double*)mem.carve(sz_f);
-  // the sweep timers, destroyed on every return path
+  if (ncp > 1 && !h->aux)
+    WT_CUDA(h, cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking));
+  // the sweep timers and the per-interval completion events of the two
+  // backward streams, destroyed on every return path
   struct Events {
-    cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
-    Events() {
-      for (cudaEvent_t& x : e) cudaEventCreate(&x);
+    std::vector<cudaEvent_t> e;
+    cudaError_t make(size_t n, unsigned flags) {
+      for (size_t k = 0; k < n; k++) {
+        cudaEvent_t x = nullptr;
+        const cudaError_t r = cudaEventCreateWithFlags(&x, flags);
+        if (r != cudaSuccess) return r;
+        e.push_back(x);
+      }
+      return cudaSuccess;
     }
     ~Events() {
       for (cudaEvent_t x : e)
         if (x) cudaEventDestroy(x);
     }
-  } ev;
+  } ev, rec_done, adj_done;
+  WT_CUDA(h, ev.make(3, cudaEventDefault));
+  WT_CUDA(h, rec_done.make((size_t)ncp, cudaEventDisableTiming));
+  WT_CUDA(h, adj_done.make((size_t)ncp, cudaEventDisableTiming));
   cudaEvent_t e0 = ev.e[0], e1 = ev.e[1], e2 = ev.e[2];
   WT_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(unsigned), h->stream));
   const dim3 grid = wt::step_grid(h->nx, h->ny, h->nz);
   const bool wide = 19 * h->n >= (1LL << 31);
-  cudaEventRecord(e0, h->stream);
+  WT_CUDA(h, cudaEventRecord(e0, h->stream));
   // forward sweep: a checkpoint every C steps, the force series for J
   for (int k = 0; k + 1 < ncp; k++) {
     WT_CUDA(h, cudaMemcpyAsync(cps + (size_t)k * pel, h->buf[h->parity], pop,
                                cudaMemcpyDeviceToDevice, h->stream));
     dispatch_steps(h, C, Path::Pbb, h->part, fdev + 3 * (size_t)k * C, h->err_dev, kChunk);
   }
-  const int tl = (ncp - 1) * C, nl = N - tl;   // the last segment
+  const int tl = (ncp - 1) * C, nl = N - tl;   // the last interval
+  S* last = seg[(ncp - 1) & 1];
   {
-    WT_CUDA(h, cudaMemcpyAsync(seg, h->buf[h->parity], pop, cudaMemcpyDeviceToDevice, h->stream));
+    WT_CUDA(h, cudaMemcpyAsync(last, h->buf[h->parity], pop, cudaMemcpyDeviceToDevice,
+                               h->stream));
     wt::StepArgs<S> fa = make_args<S>(h);
     const size_t stride = 3 * (size_t)h->nslots;
     for (int done = 0; done < nl;) {
       const int chunk = std::min(kChunk, nl - done);
       for (int s = 0; s < chunk; s++) {
-        fa.F = seg + (size_t)(done + s) * pel;
-        fa.G = seg + (size_t)(done + s + 1) * pel;
+        fa.F = last + (size_t)(done + s) * pel;
+        fa.G = last + (size_t)(done + s + 1) * pel;
         fa.part = h->part + (size_t)s * stride;
         fa.write_fields = (done + s == nl - 1) ? 1 : 0;
         launch_pbb(fa, grid, wide, h->stream);
@@ -1079,40 +1110,54 @@ int adjoint_run(wt_lattice* h, const wt_adj_cfg& cfg, int C, double* dJds, wt_ad
       h->launches++;
       done += chunk;
     }
-    WT_CUDA(h, cudaMemcpyAsync(h->buf[h->parity], seg + (size_t)nl * pel, pop,
+    WT_CUDA(h, cudaMemcpyAsync(h->buf[h->parity], last + (size_t)nl * pel, pop,
                                cudaMemcpyDeviceToDevice, h->stream));
   }
-  cudaEventRecord(e1, h->stream);
-  // backward sweep, segment by segment: recompute the segment's states from
-  // its checkpoint (the last segment's are still in the store), then run its
-  // adjoint steps last to first
+  WT_CUDA(h, cudaEventRecord(e1, h->stream));
+  // backward sweep, interval by interval from the last: the adjoint steps of
+  // interval k (last to first) on the lattice's stream, and meanwhile on the
+  // second stream the recomputation of interval k-1's states from its
+  // checkpoint into the other store. A recomputation waits for the adjoint
+  // steps that last read its store; adjoint steps wait for their states.
   WT_CUDA(h, cudaMemsetAsync(Tbuf[0], 0, tsz, h->stream));
   WT_CUDA(h, cudaMemsetAsync(ds, 0, sizeof(double) * nbox, h->stream));
   int cur = 0;   // Tbuf[cur] holds T^{t+1}
-  wt::StepArgs<S> a = make_args<S>(h);
-  a.write_fields = 0;
-  a.part = h->part;   // force partials of recomputed steps are not reduced
-  for (int k = ncp - 1; k >= 0; k--) {
+  wt::StepArgs<S> a = make_args<S>(h), r = make_args<S>(h);
+  a.write_fields = r.write_fields = 0;
+  a.part = r.part = h->part;   // force partials of recomputed steps are not reduced
+  auto adjoint_steps = [&](int k) {
     const int t0 = k * C, n = std::min(C, N - t0);
-    if (k + 1 < ncp) {
-      WT_CUDA(h, cudaMemcpyAsync(seg, cps + (size_t)k * pel, pop, cudaMemcpyDeviceToDevice,
-                                 h->stream));
-      for (int j = 0; j + 1 < n; j++) {
-        a.F = seg + (size_t)j * pel;
-        a.G = seg + (size_t)(j + 1) * pel;
-        launch_pbb(a, grid, wide, h->stream);
-        h->launches++;
-      }
-    }
+    S* sk = seg[k & 1];
     for (int t = t0 + n - 1; t >= t0; t--) {
-      a.F = seg + (size_t)(t - t0) * pel;
+      a.F = sk + (size_t)(t - t0) * pel;
       const double wJ = t >= N - W ? 1.0 / W : 0.0;
       launch_adj(a, Tbuf[cur], Tbuf[cur ^ 1], ds, wJ, cfg.component, h->stream);
       h->launches++;
       cur ^= 1;
     }
+  };
+  adjoint_steps(ncp - 1);
+  WT_CUDA(h, cudaEventRecord(adj_done.e[ncp - 1], h->stream));
+  for (int k = ncp - 2; k >= 0; k--) {
+    // recompute interval k into seg[k & 1] on the second stream
+    const int reuse = k + ns;   // the interval whose adjoint steps last read that store
+    WT_CUDA(h, cudaStreamWaitEvent(h->aux, reuse < ncp ? adj_done.e[reuse] : e1, 0));
+    S* sk = seg[k & 1];
+    WT_CUDA(h, cudaMemcpyAsync(sk, cps + (size_t)k * pel, pop, cudaMemcpyDeviceToDevice,
+                               h->aux));
+    for (int j = 0; j + 1 < C; j++) {
+      r.F = sk + (size_t)j * pel;
+      r.G = sk + (size_t)(j + 1) * pel;
+      launch_pbb(r, grid, wide, h->aux);
+      h->launches++;
+    }
+    WT_CUDA(h, cudaEventRecord(rec_done.e[k], h->aux));
+    // its adjoint steps on the lattice's stream
+    WT_CUDA(h, cudaStreamWaitEvent(h->stream, rec_done.e[k], 0));
+    adjoint_steps(k);
+    WT_CUDA(h, cudaEventRecord(adj_done.e[k], h->stream));
   }
-  cudaEventRecord(e2, h->stream);
+  WT_CUDA(h, cudaEventRecord(e2, h->stream));
   WT_CUDA(h, cudaGetLastError());
   std::vector<double> fh(3 * (size_t)N);
   WT_CUDA(h, cudaMemcpyAsync(fh.data(), fdev, sizeof(double) * fh.size(), cudaMemcpyDeviceToHost,

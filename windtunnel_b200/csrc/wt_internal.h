@@ -18,6 +18,7 @@ struct wt_lattice {
   long long pf = 0;              // L2 prefetch distance of the lean kernel (cells)
   size_t elem = 4;               // bytes per stored population
   cudaStream_t stream = nullptr;
+  cudaStream_t aux = nullptr;    // second stream of wt_adjoint (recomputation), made on first use
   void* buf[2] = {nullptr, nullptr};  // population buffers A and B (js/lbm.js:74-75)
   int parity = 0;                // js/lbm.js:80: f = parity ? B : A
   uint8_t* flags = nullptr;      // solid code (bits 0-1) | near bit (bit 2)
@@ -88,9 +89,10 @@ void launch_adj_f64(const StepArgs<double>& a, const double* Tn, double* Tc, dou
 void launch_lean_f32(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
 void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
 
-// Half storage, two adjacent cells per thread with the packed float32x2
-// collision; the lean kernel's conditions and an even nx (grid is ignored).
+// Two adjacent cells per thread with the packed float32x2 collision; the
+// lean kernel's conditions and an even nx (grid is ignored).
 void launch_pair_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
+void launch_pair_f32(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
 
 // Load the device code of every step and reduction kernel a wt_step call can
 // launch (cudaFuncGetAttributes on each), so that none is loaded lazily

@@ -26,11 +26,18 @@ void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool, cudaStream_t s)
   k_step_lean<__half><<<grid, STEP_BX, 0, s>>>(a);
 }
 
+inline dim3 pair_grid(int nx, int ny, int nz) {
+  return dim3((unsigned)((nx + 2 * PAIR_BX - 1) / (2 * PAIR_BX)), (unsigned)ny, (unsigned)nz);
+}
+
 void launch_pair_f16(const StepArgs<__half>& a, dim3, bool, cudaStream_t s) {
-  const dim3 g((unsigned)((a.nx + 2 * PAIR_BX - 1) / (2 * PAIR_BX)), (unsigned)a.ny,
-               (unsigned)a.nz);
-  if (a.f16_sr) k_step_pair<true><<<g, PAIR_BX, 0, s>>>(a);
-  else k_step_pair<false><<<g, PAIR_BX, 0, s>>>(a);
+  const dim3 g = pair_grid(a.nx, a.ny, a.nz);
+  if (a.f16_sr) k_step_pair<__half, true><<<g, PAIR_BX, 0, s>>>(a);
+  else k_step_pair<__half, false><<<g, PAIR_BX, 0, s>>>(a);
+}
+
+void launch_pair_f32(const StepArgs<float>& a, dim3, bool, cudaStream_t s) {
+  k_step_pair<float, false><<<pair_grid(a.nx, a.ny, a.nz), PAIR_BX, 0, s>>>(a);
 }
 
 // ---- partial bounce-back and adjoint (float32 arithmetic) -------------------------
@@ -119,7 +126,8 @@ cudaError_t preload_step_kernels() {
       (const void*)k_step<float, false, int>, (const void*)k_step<float, false, long long>,
       (const void*)k_step<__half, false, int>, (const void*)k_step<__half, false, long long>,
       (const void*)k_step_lean<float>, (const void*)k_step_lean<__half>,
-      (const void*)k_step_pair<false>, (const void*)k_step_pair<true>,
+      (const void*)k_step_pair<__half, false>, (const void*)k_step_pair<__half, true>,
+      (const void*)k_step_pair<float, false>,
       (const void*)k_force_reduce};
   for (const void* f : fns) {
     const cudaError_t e = cudaFuncGetAttributes(&fa, f);

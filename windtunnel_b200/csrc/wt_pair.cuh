@@ -1,5 +1,6 @@
-// wt_pair.cuh — the fused step for half storage, two adjacent cells per
-// thread, both collided at once with sm_100's packed float32x2 instructions.
+// wt_pair.cuh — the fused step, two adjacent cells per thread, both collided
+// at once with sm_100's packed float32x2 instructions (half or float32
+// storage; PairIO holds what differs between the two).
 //
 // Same semantics and per-cell rules as k_step (wt_step.cuh) and the lean
 // kernel: js/lbm.js:303-466 (stepSlab) followed by js/lbm.js:473-512
@@ -9,13 +10,16 @@
 // Thread t of block b owns cells x0 = 2 (b*PAIR_BX + t) and x0 + 1 of row
 // (y, z); nx is even, so every 32-bit word (x0, x0+1) of a population plane
 // is aligned. What the layout of the work buys, per pair of cells:
-//   * one 32-bit load per direction (the x-shifted directions add one 16-bit
-//     load of the neighbouring half at the same address +-2 bytes and a byte
-//     permute), one 32-bit store, one conversion to half pair;
+//   * one aligned load of the pair per direction (the x-shifted directions:
+//     half storage adds one 16-bit load of the neighbouring half at the same
+//     address +-2 bytes and a byte permute, float32 storage loads the
+//     straddling pair as two 4-byte words), one store of the pair (for half
+//     storage after one conversion to a half pair);
 //   * every floating-point operation of the collision issued once for both
 //     cells (FADD2 / FMUL2 / FFMA2); only the five reciprocals / square roots
 //     per cell stay scalar.
-// Registers: the 19 loaded words stay packed as half pairs. A first pass
+// Registers: the 19 loaded words stay packed (half pairs for half storage).
+// A first pass
 // converts them pair of directions by pair and accumulates the moments
 // (density, momentum, the six second moments); the equilibrium and the
 // Smagorinsky stress follow from those analytically (the D3Q19 equilibrium's
@@ -31,7 +35,7 @@
 // the first pass; solid cells keep their stale populations (pairs holding
 // one store only the other half). Rows of the edge planes and the floor row
 // (whose cells are solid or equilibrium) take their own store-only paths.
-// Conditions: half storage, float32 collision, stationary walls, nx even,
+// Conditions: half or float32 storage, float32 collision, stationary walls, nx even,
 // both population buffers under 2^31 bytes (the lean kernel's 32-bit byte
 // offsets, StepArgs srcb / dstb).
 #pragma once
@@ -41,7 +45,13 @@
 namespace wt {
 
 constexpr int PAIR_BX = 64;          // threads per block: 128 cells of one row
-constexpr int PAIR_MIN_BLOCKS = 10;  // 640 resident threads per SM: 96 registers, no spills
+// Resident blocks per SM the register budget is set for: half storage 10
+// (96 registers, no spills), float32 storage PAIR_F32_MIN_BLOCKS.
+#ifndef PAIR_F32_MIN_BLOCKS
+#define PAIR_F32_MIN_BLOCKS 8
+#endif
+template <class S>
+constexpr int pair_min_blocks() { return sizeof(S) == 2 ? 10 : PAIR_F32_MIN_BLOCKS; }
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
   return __byte_perm(a, b, sel);
@@ -82,38 +92,105 @@ __device__ __forceinline__ uint32_t put_half(uint32_t w, uint32_t v, int L) {
   return prmt(w, v, L ? 0x5410u : 0x3254u);
 }
 
+// Storage-specific pieces of the pair kernel. W is the pair (x0, x0+1) of
+// one direction as it sits in memory, R one stored element.
+template <class S>
+struct PairIO;
+
+template <>
+struct PairIO<__half> {
+  using W = uint32_t;
+  using R = uint16_t;
+  static constexpr float SC = (float)WT_F16_SCALE;
+  // (x0, x0+1) at p; (x0-1, x0) from the half at p and the word at p+2;
+  // (x0+1, x0+2) from the word at p-2 and the half at p+2
+  __device__ __forceinline__ static W load0(const char* p) { return ld32(p); }
+  __device__ __forceinline__ static W load_plus(const char* p) {
+    return prmt(ld16(p), ld32(p + 2), 0x5410u);
+  }
+  __device__ __forceinline__ static W load_minus(const char* p) {
+    return prmt(ld32(p - 2), ld16(p + 2), 0x5432u);
+  }
+  __device__ __forceinline__ static f2 to_f2(W w) { return h2f(w); }
+  __device__ __forceinline__ static W pack(f2 g) { return f2h(g); }
+  __device__ __forceinline__ static W pack_sr(f2 g, uint32_t r) { return f2h_sr(g, r); }
+  __device__ __forceinline__ static W eq(const StepArgs<__half>& a, int q) { return a.eq2[q]; }
+  __device__ __forceinline__ static W fix(W v, W e, bool inlet, bool outlet) {
+    return prmt(v, e, inlet ? 0x3254u : (outlet ? 0x1010u : 0x3210u));
+  }
+  __device__ __forceinline__ static W put(W w, R v, int L) { return put_half(w, v, L); }
+  __device__ __forceinline__ static R lane(W w, int L) { return (R)(L ? w >> 16 : w); }
+  __device__ __forceinline__ static float raw(R v) {
+    __half h;
+    memcpy(&h, &v, 2);
+    return __half2float(h);
+  }
+};
+
+template <>
+struct PairIO<float> {
+  using W = float2;
+  using R = float;
+  static constexpr float SC = 1.0f;
+  // (x0, x0+1) at p as one 8-byte load; the x-shifted pairs straddle two
+  // aligned words and are two 4-byte loads at p and p+4
+  __device__ __forceinline__ static W load0(const char* p) {
+    return *reinterpret_cast<const float2*>(p);
+  }
+  __device__ __forceinline__ static W load_plus(const char* p) {
+    return make_float2(*reinterpret_cast<const float*>(p), *reinterpret_cast<const float*>(p + 4));
+  }
+  __device__ __forceinline__ static W load_minus(const char* p) {
+    return make_float2(*reinterpret_cast<const float*>(p), *reinterpret_cast<const float*>(p + 4));
+  }
+  __device__ __forceinline__ static f2 to_f2(W w) { return w; }
+  __device__ __forceinline__ static W pack(f2 g) { return g; }
+  __device__ __forceinline__ static W pack_sr(f2 g, uint32_t) { return g; }
+  __device__ __forceinline__ static W eq(const StepArgs<float>& a, int q) {
+    return make_float2(a.eq[q], a.eq[q]);
+  }
+  __device__ __forceinline__ static W fix(W v, W e, bool inlet, bool outlet) {
+    return make_float2(inlet ? e.x : v.x, outlet ? v.x : v.y);
+  }
+  __device__ __forceinline__ static W put(W w, R v, int L) {
+    return L ? make_float2(w.x, v) : make_float2(v, w.y);
+  }
+  __device__ __forceinline__ static R lane(W w, int L) { return L ? w.y : w.x; }
+  __device__ __forceinline__ static float raw(R v) { return v; }
+};
+
 // Re-gather the bounce-back and free-slip directions of cell xL = x0 + L (raw
 // half bits into half L of each word), js/lbm.js:334-368 for the bounce-back
 // links (stationary walls). The momentum exchange of body links accumulates
 // in float64 in raw units.
-__device__ __forceinline__ void pair_patch(const StepArgs<__half>& a, long long iL, int xL, int y,
+template <class S>
+__device__ __forceinline__ void pair_patch(const StepArgs<S>& a, long long iL, int xL, int y,
                                            int z, bool near_cell, bool shell, int L,
-                                           uint32_t (&w)[Q], double& Fx, double& Fy,
-                                           double& Fz) {
+                                           typename PairIO<S>::W (&w)[Q], double& Fx,
+                                           double& Fy, double& Fz) {
+  using IO = PairIO<S>;
+  using R = typename IO::R;
   const unsigned long long m = near_cell ? a.nmask[iL] : 0ull;
   const unsigned sm = (unsigned)m, om = (unsigned)(m >> 32);
-  const uint16_t* F = reinterpret_cast<const uint16_t*>(a.F);
+  const R* F = reinterpret_cast<const R*>(a.F);
 #define WT_PAIR_PATCH(q)                                                                   \
   if ((sm >> (q)) & 1u) {                                                                  \
-    const uint32_t v = F[opp(q) * a.n + iL];                                               \
+    const R v = F[opp(q) * a.n + iL];                                                      \
     if ((om >> (q)) & 1u) {                                                                \
-      __half hv;                                                                           \
-      const uint16_t hb = (uint16_t)v;                                                     \
-      memcpy(&hv, &hb, 2);                                                                 \
-      const float d = 2.0f * __half2float(hv);                                             \
+      const float d = 2.0f * IO::raw(v);                                                   \
       Fx -= (double)(d * (float)ex(q));                                                    \
       Fy -= (double)(d * (float)ey(q));                                                    \
       Fz -= (double)(d * (float)ez(q));                                                    \
     }                                                                                      \
-    w[q] = put_half(w[q], v, L);                                                           \
+    w[q] = IO::put(w[q], v, L);                                                            \
   } else if (shell) {                                                                      \
     int sy = y - ey(q), sz = z - ez(q), qq = q;                                            \
     bool refl = false;                                                                     \
     if (sy == 0 || sy == a.ny - 1) { sy = y; qq = mirror_y(qq); refl = true; }             \
     if (sz == 0 || sz == a.nz - 1) { sz = z; qq = mirror_z(qq); refl = true; }             \
     if (refl)                                                                              \
-      w[q] = put_half(w[q], F[qq * a.n + (xL - ex(q)) + (long long)a.nx * sy + a.nxy * sz], \
-                      L);                                                                  \
+      w[q] = IO::put(w[q], F[qq * a.n + (xL - ex(q)) + (long long)a.nx * sy + a.nxy * sz], \
+                     L);                                                                   \
   }
   WT_PAIR_PATCH(1) WT_PAIR_PATCH(2) WT_PAIR_PATCH(3) WT_PAIR_PATCH(4) WT_PAIR_PATCH(5)
   WT_PAIR_PATCH(6) WT_PAIR_PATCH(7) WT_PAIR_PATCH(8) WT_PAIR_PATCH(9) WT_PAIR_PATCH(10)
@@ -126,8 +203,9 @@ __device__ __forceinline__ void pair_patch(const StepArgs<__half>& a, long long 
 // segments (lanes 0-15 and 16-31). Each half-warp that holds a near-wall
 // cell sums its doubles in a fixed order and its first lane stores them in
 // the segment's slot. Every lane must call it.
+template <class S>
 __device__ __forceinline__ void pair_force_partial(double fx, double fy, double fz,
-                                                   bool near_cell, const StepArgs<__half>& a) {
+                                                   bool near_cell, const StepArgs<S>& a) {
   const unsigned any = __ballot_sync(0xffffffffu, near_cell);
   if (any == 0u) return;
 #pragma unroll
@@ -151,10 +229,13 @@ __device__ __forceinline__ void pair_force_partial(double fx, double fy, double 
   }
 }
 
-template <bool SR>
-__global__ void __launch_bounds__(PAIR_BX, PAIR_MIN_BLOCKS)
-    k_step_pair(const __grid_constant__ StepArgs<__half> a) {
-  constexpr float SC = (float)WT_F16_SCALE;
+template <class S, bool SR>
+__global__ void __launch_bounds__(PAIR_BX, pair_min_blocks<S>())
+    k_step_pair(const __grid_constant__ StepArgs<S> a) {
+  using IO = PairIO<S>;
+  using W = typename IO::W;
+  using R = typename IO::R;
+  constexpr float SC = IO::SC;
   const int x0 = 2 * (blockIdx.x * PAIR_BX + threadIdx.x);
   const int y = blockIdx.y, z = blockIdx.z;
   const long long i0 = (long long)x0 + (long long)a.nx * y + a.nxy * z;
@@ -162,14 +243,14 @@ __global__ void __launch_bounds__(PAIR_BX, PAIR_MIN_BLOCKS)
   bool near_out = false;
   if (x0 < a.nx) {
     char* Gb = reinterpret_cast<char*>(a.G + i0);
-    auto gw = [&](int q) -> uint32_t& { return *reinterpret_cast<uint32_t*>(Gb + a.dstb[q]); };
-    auto gh = [&](int q, int L) -> uint16_t& {
-      return *reinterpret_cast<uint16_t*>(Gb + a.dstb[q] + 2 * L);
+    auto gw = [&](int q) -> W& { return *reinterpret_cast<W*>(Gb + a.dstb[q]); };
+    auto gh = [&](int q, int L) -> R& {
+      return *reinterpret_cast<R*>(Gb + a.dstb[q] + sizeof(R) * L);
     };
     if (z == 0 || z == a.nz - 1 || y == a.ny - 1) {
       // end planes and ceiling: the free-stream equilibrium (js/lbm.js:490-503)
 #pragma unroll
-      for (int q = 0; q < Q; q++) gw(q) = a.eq2[q];
+      for (int q = 0; q < Q; q++) gw(q) = IO::eq(a, q);
       if (a.write_fields) {
         *reinterpret_cast<float2*>(a.ux + i0) = make_float2(a.u0f, a.u0f);
         *reinterpret_cast<float2*>(a.uy + i0) = make_float2(0.f, 0.f);
@@ -197,7 +278,7 @@ __global__ void __launch_bounds__(PAIR_BX, PAIR_MIN_BLOCKS)
           continue;
         }
 #pragma unroll
-        for (int q = 0; q < Q; q++) gh(q, L) = (uint16_t)a.eq2[q];
+        for (int q = 0; q < Q; q++) gh(q, L) = IO::lane(IO::eq(a, q), 0);
         if (a.write_fields) {
           a.ux[i0 + L] = a.u0f; a.uy[i0 + L] = 0.f; a.uz[i0 + L] = 0.f; a.rho[i0 + L] = 1.f;
         }
@@ -207,19 +288,13 @@ __global__ void __launch_bounds__(PAIR_BX, PAIR_MIN_BLOCKS)
       // the pair (x0 - ex, x0 + 1 - ex) of row (y - ey, z - ez) lie inside
       // the buffer for every cell of an interior row.
       const char* Fb = reinterpret_cast<const char*>(a.F + i0);
-      uint32_t w[Q];
+      W w[Q];
 #define WT_PAIR_LOAD(q)                                                                  \
   {                                                                                      \
     const char* p = Fb + a.srcb[q];   /* byte address of the source of cell x0 */        \
-    if constexpr (ex(q) == 0) {                                                          \
-      w[q] = ld32(p);                                                                    \
-    } else if constexpr (ex(q) == 1) {                                                   \
-      /* (x0-1, x0): the half at p, then the low half of the word at p+2 */              \
-      w[q] = prmt(ld16(p), ld32(p + 2), 0x5410u);                                        \
-    } else {                                                                             \
-      /* (x0+1, x0+2): the high half of the word at p-2, then the half at p+2 */         \
-      w[q] = prmt(ld32(p - 2), ld16(p + 2), 0x5432u);                                    \
-    }                                                                                    \
+    if constexpr (ex(q) == 0) w[q] = IO::load0(p);                                       \
+    else if constexpr (ex(q) == 1) w[q] = IO::load_plus(p);                              \
+    else w[q] = IO::load_minus(p);                                                       \
   }
       WT_PAIR_LOAD(0) WT_PAIR_LOAD(1) WT_PAIR_LOAD(2) WT_PAIR_LOAD(3) WT_PAIR_LOAD(4)
       WT_PAIR_LOAD(5) WT_PAIR_LOAD(6) WT_PAIR_LOAD(7) WT_PAIR_LOAD(8) WT_PAIR_LOAD(9)
@@ -248,30 +323,30 @@ __global__ void __launch_bounds__(PAIR_BX, PAIR_MIN_BLOCKS)
       // ---- pass 1: moments --------------------------------------------------
       f2 dr, jx, jy, jz, pxx, pyy, pzz, pxy, pxz, pyz;
       {
-        const f2 f0 = h2f(w[0]);
-        f2 fa = h2f(w[1]), fb = h2f(w[2]);
+        const f2 f0 = IO::to_f2(w[0]);
+        f2 fa = IO::to_f2(w[1]), fb = IO::to_f2(w[2]);
         f2 s = padd(fa, fb), d = psub(fa, fb);
         dr = padd(f0, s); jx = d; pxx = s;
-        fa = h2f(w[3]); fb = h2f(w[4]); s = padd(fa, fb); d = psub(fa, fb);
+        fa = IO::to_f2(w[3]); fb = IO::to_f2(w[4]); s = padd(fa, fb); d = psub(fa, fb);
         dr = padd(dr, s); jy = d; pyy = s;
-        fa = h2f(w[5]); fb = h2f(w[6]); s = padd(fa, fb); d = psub(fa, fb);
+        fa = IO::to_f2(w[5]); fb = IO::to_f2(w[6]); s = padd(fa, fb); d = psub(fa, fb);
         dr = padd(dr, s); jz = d; pzz = s;
-        fa = h2f(w[7]); fb = h2f(w[8]); s = padd(fa, fb); d = psub(fa, fb);
+        fa = IO::to_f2(w[7]); fb = IO::to_f2(w[8]); s = padd(fa, fb); d = psub(fa, fb);
         dr = padd(dr, s); jx = padd(jx, d); jy = padd(jy, d); pxx = padd(pxx, s);
         pyy = padd(pyy, s); pxy = s;
-        fa = h2f(w[9]); fb = h2f(w[10]); s = padd(fa, fb); d = psub(fa, fb);
+        fa = IO::to_f2(w[9]); fb = IO::to_f2(w[10]); s = padd(fa, fb); d = psub(fa, fb);
         dr = padd(dr, s); jx = padd(jx, d); jy = psub(jy, d); pxx = padd(pxx, s);
         pyy = padd(pyy, s); pxy = psub(pxy, s);
-        fa = h2f(w[11]); fb = h2f(w[12]); s = padd(fa, fb); d = psub(fa, fb);
+        fa = IO::to_f2(w[11]); fb = IO::to_f2(w[12]); s = padd(fa, fb); d = psub(fa, fb);
         dr = padd(dr, s); jx = padd(jx, d); jz = padd(jz, d); pxx = padd(pxx, s);
         pzz = padd(pzz, s); pxz = s;
-        fa = h2f(w[13]); fb = h2f(w[14]); s = padd(fa, fb); d = psub(fa, fb);
+        fa = IO::to_f2(w[13]); fb = IO::to_f2(w[14]); s = padd(fa, fb); d = psub(fa, fb);
         dr = padd(dr, s); jx = padd(jx, d); jz = psub(jz, d); pxx = padd(pxx, s);
         pzz = padd(pzz, s); pxz = psub(pxz, s);
-        fa = h2f(w[15]); fb = h2f(w[16]); s = padd(fa, fb); d = psub(fa, fb);
+        fa = IO::to_f2(w[15]); fb = IO::to_f2(w[16]); s = padd(fa, fb); d = psub(fa, fb);
         dr = padd(dr, s); jy = padd(jy, d); jz = padd(jz, d); pyy = padd(pyy, s);
         pzz = padd(pzz, s); pyz = s;
-        fa = h2f(w[17]); fb = h2f(w[18]); s = padd(fa, fb); d = psub(fa, fb);
+        fa = IO::to_f2(w[17]); fb = IO::to_f2(w[18]); s = padd(fa, fb); d = psub(fa, fb);
         dr = padd(dr, s); jy = padd(jy, d); jz = psub(jz, d); pyy = padd(pyy, s);
         pzz = padd(pzz, s); pyz = psub(pyz, s);
       }
@@ -345,43 +420,43 @@ __global__ void __launch_bounds__(PAIR_BX, PAIR_MIN_BLOCKS)
       const f2 k45f = pmul(pk(0.25f), omr), k45e = pmul(pk(0.125f), omr);
       const f2 kaf = pmul(pk((float)(1.0 / 18)), omA), kae = pmul(pk((float)(1.0 / 36)), omA);
       const f2 k3f = pmul(pk((float)(1.0 / 6)), ommr), k3e = pmul(pk((float)(1.0 / 12)), ommr);
-      // store selection: the inlet's low half takes the equilibrium, the
-      // outlet's high half takes cell nx-2's half
-      const uint32_t sel = inlet ? 0x3254u : (outlet ? 0x1010u : 0x3210u);
       // a solid cell keeps its stale populations, and so does the outlet copy
       // of a solid cell nx-2 until the copy below
       const bool keep0 = solid0 && !inlet, keep1 = solid1 || (outlet && solid0);
       const bool keep_any = keep0 || keep1;
+      // stochastic rounding: a hash of (pair, step), then per output word its
+      // product with a distinct odd constant (one multiply per word)
       uint32_t h = 0;
       if constexpr (SR) {
         h = ((uint32_t)i0 ^ (uint32_t)(i0 >> 32)) * 0x9E3779B1u ^ a.sr_seed;
         h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
       }
       auto put = [&](int q, f2 g) {
-        uint32_t v;
+        W v;
         if constexpr (SR) {
-          h ^= h << 13; h ^= h >> 17; h ^= h << 5;
-          v = f2h_sr(g, h);
+          v = IO::pack_sr(g, h * (0x9E3779B1u * (2u * (uint32_t)q + 1u)));
         } else {
-          v = f2h(g);
+          v = IO::pack(g);
         }
-        v = prmt(v, a.eq2[q], sel);
+        // the inlet's low cell takes the equilibrium, the outlet's high cell
+        // takes cell nx-2's value
+        v = IO::fix(v, IO::eq(a, q), inlet, outlet);
         if (!keep_any) {
           gw(q) = v;
         } else {
           // a solid cell of the pair keeps its stale population
-          if (!keep0) gh(q, 0) = (uint16_t)v;
-          if (!keep1) gh(q, 1) = (uint16_t)(v >> 16);
+          if (!keep0) gh(q, 0) = IO::lane(v, 0);
+          if (!keep1) gh(q, 1) = IO::lane(v, 1);
         }
       };
       // ---- pass 2: outputs ----------------------------------------------------
       {
-        const f2 f0 = h2f(w[0]);
+        const f2 f0 = IO::to_f2(w[0]);
         put(0, pfma(pfma(pk(-1.0f), om, pk(1.0f)), f0, pmul(pk((float)(1.0 / 3)), omA)));
       }
 #define WT_PAIR_OUT(qa, C, K45, KA, K3)                 \
   {                                                     \
-    const f2 fa = h2f(w[qa]), fb = h2f(w[qa + 1]);      \
+    const f2 fa = IO::to_f2(w[qa]), fb = IO::to_f2(w[qa + 1]);      \
     const f2 s = padd(fa, fb), d = psub(fa, fb);        \
     const f2 c = C;                                     \
     const f2 X = pfma(pmul(c, c), K45, KA);             \
