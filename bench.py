@@ -328,7 +328,7 @@ def accuracy_study(wl, replicas: int = 4, steps: int | None = None,
            "seeds": [wl["seed"] + k for k in range(replicas)],
            "statistic": "mean over seeded replicas of the pair-averaged coefficient over "
                         "the last `window` steps; sem = std / sqrt(replicas)"}
-    per = {}
+    per, first = {}, {}
     for name, storage, mm, rounding in ACCURACY_FORMS:
         sim = setup_gpu(wl, storage, mm)
         if rounding:
@@ -341,6 +341,8 @@ def accuracy_study(wl, replicas: int = 4, steps: int | None = None,
             c = window_coefficients(F, wl["u0"], sim.frontalArea, window)
             cd.append(c["cd"])
             cl.append(c["cl"])
+            if k == 0:
+                first[name] = (F, sim.frontalArea)
         sim.close()
         per[name] = (np.array(cd), np.array(cl))
         e = {"cd": float(np.mean(cd)), "cl": float(np.mean(cl)),
@@ -350,6 +352,22 @@ def accuracy_study(wl, replicas: int = 4, steps: int | None = None,
         if rounding:
             e["rounding"] = rounding
         out[name] = e
+    # the storage error before the flow separates the trajectories: the
+    # first seed's pair-averaged Cd over consecutive 500-step windows, every
+    # form against float64 from the same initial state
+    F64, area = first["f64"]
+    q = 0.5 * wl["u0"] ** 2 * area
+    def wcd(F, a, b):
+        pa = 0.5 * (F[1:, 0] + F[:-1, 0])
+        return float(pa[a:b].mean() / q)
+    rows = []
+    for a in range(0, steps - 1, 500):
+        b = min(a + 500, steps - 1)
+        ref = wcd(F64, a, b)
+        rows.append({"steps": [a, b + 1], "cd_f64": ref,
+                     **{f"dcd_rel_{n}": (wcd(first[n][0], a, b) - ref) / abs(ref)
+                        for n in first if n != "f64"}})
+    out["seed0_windows"] = rows
     for ref in ("f64", "f32"):
         rcd, rcl = per[ref]
         for name, (cd, cl) in per.items():
