@@ -721,16 +721,16 @@ def run_wt(args) -> None:
         return BYTES_PER_CELL[form] * n * K / (t_ms * 1e-3) / 1e9
 
     a32, a16 = achieved("f32", ms), achieved("f16dev", ms16)
-    traffic = profiled_traffic(f"k_step_lean_f32_{wl['nx']}x{wl['ny']}x{wl['nz']}")
-    kern16 = "pair" if (ROOT / "profiles" / f"k_step_pair_f16_{wl['nx']}x{wl['ny']}x{wl['nz']}.md"
-                        ).exists() else "lean"
+    shape = f"{wl['nx']}x{wl['ny']}x{wl['nz']}"
+    traffic = profiled_traffic(f"k_step_pair_f32_{shape}")
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": dist.world,
         "steps": K, "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(wl, dist.world),
-        "kernel": "lean (one thread per cell, 32-bit offsets; WT_KERNEL_AUTO), float32 "
-                  "collision (WT_MATH_FAST)",
+        "kernel": "pair (two cells per thread, one aligned load and store of the pair per "
+                  "direction, packed float32x2 collision; WT_KERNEL_AUTO), float32 collision "
+                  "(WT_MATH_FAST)",
         "roofline": {"bound": "hbm", "achieved": round(a32, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(a32 / peak, 4), "traffic": traffic,
                      "peak_source": peak_kind,
@@ -740,7 +740,7 @@ def run_wt(args) -> None:
                      "fp16dev_frac": round(a16 / peak, 4),
                      "fp16dev_bytes_per_cell": BYTES_PER_CELL["f16dev"],
                      "fp16dev_traffic": profiled_traffic(
-                         f"k_step_{kern16}_f16_{wl['nx']}x{wl['ny']}x{wl['nz']}")},
+                         f"k_step_pair_f16_{shape}")},
         "e2e": {"value": round(e2e_val, 1), "unit": "MLUPS",
                 "h2d_bytes_per_step": h2d / 16, "d2h_bytes_per_step": 3 * 8 + 4 / 16,
                 "steps": ke,

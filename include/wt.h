@@ -74,8 +74,8 @@ enum {
  * measured slower than LEAN on B200 and were removed; they are not reused
  * and are rejected (WT_ERR_ARG). */
 enum {
-  WT_KERNEL_AUTO = 0,    /* the kernel measured fastest on B200 for the form: PAIR for half
-                            storage when it can run, else LEAN when it can run, else DIRECT */
+  WT_KERNEL_AUTO = 0,    /* the kernel measured fastest on B200 for the form: PAIR when it
+                            can run, else LEAN when it can run, else DIRECT */
   WT_KERNEL_DIRECT = 1,  /* one thread per cell, populations gathered straight from HBM;
                             every storage, arithmetic and boundary option */
   WT_KERNEL_LEAN = 7,    /* one thread per cell, 32-bit byte offsets from one pointer per cell,

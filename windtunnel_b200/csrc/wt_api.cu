@@ -211,12 +211,13 @@ bool lean_ok(const wt_lattice* h);
 bool pair_ok(const wt_lattice* h);
 
 // The kernel WT_KERNEL_AUTO runs, the fastest measured on B200 for the form
-// (256x128x128 channel): the lean kernel where it can run (float32 36.7k
-// MLUPS against 33.3k for the direct kernel; half, with its L2 prefetch,
-// 44.3k against 37.2k), the direct kernel otherwise (exact collision,
-// float64, moving walls, buffers of 2^31 bytes or more).
+// (256x128x128 channel, 1000-step calls): the pair kernel where it can run
+// (float32 storage 40.3k MLUPS against 37.9k for the lean kernel; half
+// storage 55.2k against 44.4k), the lean kernel for an odd nx, the direct
+// kernel otherwise (exact collision, float64, moving walls, buffers of 2^31
+// bytes or more).
 Path auto_path(const wt_lattice* h) {
-  if (h->storage == WT_STORE_F16DEV && pair_ok(h)) return Path::Pair;
+  if (pair_ok(h)) return Path::Pair;
   if (lean_ok(h)) return Path::Lean;
   return Path::Direct;
 }
