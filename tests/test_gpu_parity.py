@@ -346,11 +346,12 @@ def test_lean_stochastic_rounding_agrees_with_direct(both):
     assert np.abs(pa - pb).max() <= 1e-4
 
 
+@pytest.mark.parametrize("kernel", ["lean", "pair"])
 @pytest.mark.parametrize("storage", ["f32", "f16dev"])
-def test_lean_prefetch_changes_nothing(both, storage, monkeypatch):
-    """The lean kernel's L2 prefetch distance (read at create time) moves
-    timing only: off, the default and one past the end of the lattice give
-    bit-identical populations and forces."""
+def test_prefetch_changes_nothing(both, storage, kernel, monkeypatch):
+    """The L2 prefetch distance of the lean and pair kernels (read at create
+    time) moves timing only: off, the default and one past the end of the
+    lattice give bit-identical populations and forces."""
     LBM, _ = both
     dims = (64, 20, 18)
     out = []
@@ -359,7 +360,7 @@ def test_lean_prefetch_changes_nothing(both, storage, monkeypatch):
             monkeypatch.delenv("WT_PREFETCH_CELLS", raising=False)
         else:
             monkeypatch.setenv("WT_PREFETCH_CELLS", pf)
-        s = LBM(*dims, storage=storage, kernel="lean", side_bc="freeslip")
+        s = LBM(*dims, storage=storage, kernel=kernel, side_bc="freeslip")
         apply_case(s, sphere=(40.0, 10.0, 9.0, 4.2), side_bc="freeslip", ground=True)
         out.append((s.step_forces(25), s.populations("f", "raw")))
     monkeypatch.delenv("WT_PREFETCH_CELLS", raising=False)

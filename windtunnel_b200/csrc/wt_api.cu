@@ -339,14 +339,15 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
   h->stats.frontal_area = 1;
   cudaGetDevice(&h->device);
   {
-    // The lean kernel can prefetch into L2 the populations of the warp this
-    // many cells further on in launch order: a third of the cells its
-    // resident blocks (8 per SM) cover. Measured on B200 it pays only for half
-    // storage on lattices whose population buffer fits in twice the L2
-    // (256x128x128: +7% over none, flat from 0.15 to 0.65 of the resident
-    // cells); it cost 8% for float32 storage on the same lattice and 19% for
-    // half storage on 512x192x192, whatever the distance, so it is off there.
-    // WT_PREFETCH_CELLS overrides it (0: off).
+    // The lean and pair kernels can prefetch into L2 the populations of the
+    // warp this many cells further on in launch order: a third of the cells
+    // the lean kernel's resident blocks (8 per SM) cover. Measured on B200 it
+    // pays only for half storage on lattices whose population buffer fits in
+    // twice the L2 (256x128x128: lean +7% over none, flat from 0.15 to 0.65 of
+    // the resident cells; pair +3%); it cost the lean kernel 8% for float32
+    // storage on the same lattice and 19% for half storage on 512x192x192,
+    // whatever the distance, so it is off there. WT_PREFETCH_CELLS overrides it
+    // (0: off).
     int sms = 0, l2 = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
     cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, h->device);

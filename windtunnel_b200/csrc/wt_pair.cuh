@@ -503,6 +503,9 @@ __global__ void __launch_bounds__(PAIR_BX, pair_min_blocks<S>())
   // interior row: pull every direction of both cells. The sources of the
   // pair (x0 - ex, x0 + 1 - ex) of row (y - ey, z - ez) lie inside the
   // buffer for every cell of an interior row.
+  // L2 prefetch of the populations the warp a fixed distance ahead will
+  // pull (StepArgs pf; set for half storage on lattices within twice the L2)
+  prefetch_ahead(a, i0 - 2 * (long long)(threadIdx.x & 31));
   const char* Fb = reinterpret_cast<const char*>(a.F + i0);
   W w[Q];
   if (active) {
