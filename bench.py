@@ -381,6 +381,82 @@ def accuracy_study(wl, replicas: int = 4, steps: int | None = None,
     return out
 
 
+def long_window_accuracy(wl, steps: int, spinup: int | None = None, block: int = 10000,
+                         forms: list[str] | None = None) -> dict:
+    """Cd / Cl of each storage form over one long window, against float64.
+
+    One trajectory per form from the first seed: `spinup` steps (the
+    configuration's step count) and then `steps` steps whose pair-averaged
+    drag and lift (js/main.js:113-127) are summed into blocks of `block`
+    steps. A form's Cd is the mean over its blocks; its standard error is
+    std(block means) / sqrt(blocks), the batch-means estimate behind the
+    reference's blocking SEM (js/main.js:163-212), given for block lengths 1,
+    2, 5 and 10 times `block` so that its plateau shows that the blocks are
+    long enough to be independent. The forms' trajectories separate within
+    the spin-up, so the error of a form against float64 (or float32) has the
+    standard error sqrt(sem_a^2 + sem_b^2). Each form's entry is printed
+    to stderr as it completes."""
+    import numpy as np
+
+    spinup = wl["accuracy_steps"] if spinup is None else spinup
+    nb = steps // block
+    steps = nb * block
+    chunk = block * max(1, 200000 // block)
+    out = {"workload": wl["name"], "seed": wl["seed"], "spinup": spinup, "steps": steps,
+           "block": block,
+           "statistic": "pair-averaged coefficient over `steps` steps after `spinup`; sem = "
+                        "std(block means) / sqrt(blocks)"}
+    per = {}
+    for name, storage, mm, rounding in ACCURACY_FORMS:
+        if forms and name not in forms:
+            continue
+        sim = setup_gpu(wl, storage, mm)
+        if rounding:
+            sim.set_params(f16_rounding=rounding)
+        q = 0.5 * wl["u0"] ** 2 * sim.frontalArea
+        t0 = time.time()
+        last = sim.step_forces(spinup)[-1] if spinup else np.zeros(3)
+        sums = np.zeros((nb, 2))
+        done = 0
+        while done < steps:
+            F = sim.step_forces(min(chunk, steps - done))
+            pa = 0.5 * (F + np.vstack([last[None, :], F[:-1]]))
+            sums[done // block:(done + len(F)) // block] = \
+                pa[:, :2].reshape(-1, block, 2).sum(axis=1)
+            last = F[-1]
+            done += len(F)
+        sim.close()
+        means = sums / (block * q)
+        cd = float(means[:, 0].mean())
+        cl = float(means[:, 1].mean())
+
+        def sem(col, m):
+            k = nb // m
+            if k < 2:
+                return None
+            b = col[:k * m].reshape(k, m).mean(axis=1)
+            return float(np.std(b, ddof=1) / math.sqrt(k))
+        e = {"cd": cd, "cl": cl, "cd_sem": sem(means[:, 0], 1), "cl_sem": sem(means[:, 1], 1),
+             "cd_sem_by_block": {str(m * block): sem(means[:, 0], m) for m in (1, 2, 5, 10)},
+             "wall_s": round(time.time() - t0, 1)}
+        if rounding:
+            e["rounding"] = rounding
+        per[name] = e
+        out[name] = e
+        print(json.dumps({name: e}), file=sys.stderr, flush=True)
+    for ref in ("f64", "f32"):
+        if ref not in per:
+            continue
+        r = per[ref]
+        for name, e in per.items():
+            if name == ref or (ref == "f32" and name == "f64"):
+                continue
+            e[f"dcd_rel_vs_{ref}"] = (e["cd"] - r["cd"]) / abs(r["cd"])
+            e[f"dcd_rel_vs_{ref}_sem"] = math.hypot(e["cd_sem"], r["cd_sem"]) / abs(r["cd"])
+            e[f"dcl_vs_{ref}_over_cd"] = (e["cl"] - r["cl"]) / abs(r["cd"])
+    return out
+
+
 def steady_accuracy(wl) -> dict:
     """The storage error alone, on a steady wake: one run per form, Cd / Cl
     over the last window steps against float64 storage."""
@@ -836,12 +912,16 @@ def run_reference(args) -> None:
 
 def run_study(args) -> None:
     """`--study accuracy`: the accuracy ensemble on --workload with --replicas
-    seeds per form; `--study adjoint-horizon`: the half-vs-float32 gradient
+    seeds per form; `--study accuracy-long`: one --long-steps window per form
+    (--forms); `--study adjoint-horizon`: the half-vs-float32 gradient
     agreement of the 384x160x160 differentiation workload against horizon."""
     import torch
     torch.cuda.set_device(0)
     if args.study == "accuracy":
         res = accuracy_study(WORKLOADS[args.workload], replicas=args.replicas)
+    elif args.study == "accuracy-long":
+        res = long_window_accuracy(WORKLOADS[args.workload], args.long_steps,
+                                   forms=args.forms.split(",") if args.forms else None)
     else:
         res = adjoint_horizon_study(ADJOINT_WORKLOADS["design384"])
     print(json.dumps(res), flush=True)
@@ -857,8 +937,13 @@ def main() -> None:
     ap.add_argument("--no-accuracy", dest="accuracy", action="store_false")
     ap.add_argument("--replicas", type=int, default=4,
                     help="seeded replicas per storage form in the accuracy ensemble")
-    ap.add_argument("--study", choices=["accuracy", "adjoint-horizon"],
+    ap.add_argument("--study", choices=["accuracy", "accuracy-long", "adjoint-horizon"],
                     help="run one study alone and print its JSON (no timing line)")
+    ap.add_argument("--long-steps", type=int, default=3000000,
+                    help="averaged steps per form of --study accuracy-long")
+    ap.add_argument("--forms", default=None,
+                    help="comma-separated storage forms of --study accuracy-long "
+                         "(f64,f32,f16dev,f16dev_stochastic; default all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
     ap.add_argument("--no-adjoint-scale", dest="adjoint_scale", action="store_false")
