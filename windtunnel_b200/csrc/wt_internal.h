@@ -94,6 +94,10 @@ void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream
 void launch_pair_f16(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s);
 void launch_pair_f32(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s);
 
+// Launch attributes of the step kernels (the pair kernels' L1 carveout), set
+// once per lattice creation.
+cudaError_t configure_step_kernels();
+
 // Load the device code of every step and reduction kernel a wt_step call can
 // launch (cudaFuncGetAttributes on each), so that none is loaded lazily
 // inside a later call. The exact variant covers the --fmad=false unit.

@@ -120,6 +120,21 @@ void launch_force_reduce(const double* part, unsigned nslots, int nsteps, double
   k_force_reduce<<<nsteps, RED_T, 0, s>>>(part, nslots, out);
 }
 
+cudaError_t configure_step_kernels() {
+  // The pair kernels use no shared memory: the whole unified L1 / shared
+  // array goes to L1 (measured on B200: +1.6% for half storage on
+  // 256x128x128, +0.5% on 512x192x192, float32 unchanged).
+  const void* fns[] = {(const void*)k_step_pair<__half, false>,
+                       (const void*)k_step_pair<__half, true>,
+                       (const void*)k_step_pair<float, false>};
+  for (const void* f : fns) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t preload_step_kernels() {
   cudaFuncAttributes fa;
   const void* fns[] = {
