@@ -358,8 +358,14 @@ int wt_create(int nx, int ny, int nz, int storage, wt_lattice** out) {
   }
   h->nsegs = (long long)((nx + 31) / 32) * ny * nz;
   const size_t pop = (size_t)n * 19 * h->elem;
+  if (const cudaError_t e = wt::configure_step_kernels(); e != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    g_create_error = std::string("setting the step kernels' attributes failed: ") +
+                     cudaGetErrorString(e);
+    return WT_ERR_CUDA;
+  }
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
-  ok = ok && wt::configure_step_kernels() == cudaSuccess;
   ok = ok && cudaMalloc(&h->buf[0], pop) == cudaSuccess;
   ok = ok && cudaMalloc(&h->buf[1], pop) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&h->flags, (size_t)n) == cudaSuccess;
