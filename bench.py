@@ -382,10 +382,11 @@ def accuracy_study(wl, replicas: int = 4, steps: int | None = None,
 
 
 def long_window_accuracy(wl, steps: int, spinup: int | None = None, block: int = 10000,
-                         forms: list[str] | None = None) -> dict:
+                         forms: list[str] | None = None, noise_seed: int | None = None) -> dict:
     """Cd / Cl of each storage form over one long window, against float64.
 
-    One trajectory per form from the first seed: `spinup` steps (the
+    One trajectory per form from the workload's seed (or `noise_seed` for the
+    initial velocity noise, the body unchanged): `spinup` steps (the
     configuration's step count) and then `steps` steps whose pair-averaged
     drag and lift (js/main.js:113-127) are summed into blocks of `block`
     steps. A form's Cd is the mean over its blocks; its standard error is
@@ -402,7 +403,8 @@ def long_window_accuracy(wl, steps: int, spinup: int | None = None, block: int =
     nb = steps // block
     steps = nb * block
     chunk = block * max(1, 200000 // block)
-    out = {"workload": wl["name"], "seed": wl["seed"], "spinup": spinup, "steps": steps,
+    seed = wl["seed"] if noise_seed is None else noise_seed
+    out = {"workload": wl["name"], "seed": seed, "spinup": spinup, "steps": steps,
            "block": block,
            "statistic": "pair-averaged coefficient over `steps` steps after `spinup`; sem = "
                         "std(block means) / sqrt(blocks)"}
@@ -413,6 +415,8 @@ def long_window_accuracy(wl, steps: int, spinup: int | None = None, block: int =
         sim = setup_gpu(wl, storage, mm)
         if rounding:
             sim.set_params(f16_rounding=rounding)
+        if noise_seed is not None:
+            sim.init_eq_noise(noise_seed, wl["amp"])
         q = 0.5 * wl["u0"] ** 2 * sim.frontalArea
         t0 = time.time()
         last = sim.step_forces(spinup)[-1] if spinup else np.zeros(3)
@@ -927,7 +931,8 @@ def run_study(args) -> None:
         res = accuracy_study(WORKLOADS[args.workload], replicas=args.replicas)
     elif args.study == "accuracy-long":
         res = long_window_accuracy(WORKLOADS[args.workload], args.long_steps,
-                                   forms=args.forms.split(",") if args.forms else None)
+                                   forms=args.forms.split(",") if args.forms else None,
+                                   noise_seed=args.seed)
     else:
         res = adjoint_horizon_study(ADJOINT_WORKLOADS["design384"])
     print(json.dumps(res), flush=True)
@@ -947,6 +952,9 @@ def main() -> None:
                     help="run one study alone and print its JSON (no timing line)")
     ap.add_argument("--long-steps", type=int, default=3000000,
                     help="averaged steps per form of --study accuracy-long")
+    ap.add_argument("--seed", type=int, default=None,
+                    help="initial velocity-noise seed of --study accuracy-long (the body "
+                         "stays the workload's; default: the workload's seed)")
     ap.add_argument("--forms", default=None,
                     help="comma-separated storage forms of --study accuracy-long "
                          "(f64,f32,f16dev,f16dev_stochastic; default all)")

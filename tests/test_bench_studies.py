@@ -30,6 +30,9 @@ class FakeLattice:
     def set_params(self, **_):
         pass
 
+    def init_eq_noise(self, seed, amp):
+        self.noise = (seed, amp)
+
     def step_forces(self, n):
         t = np.arange(self.t, self.t + n, dtype=np.float64)
         F = np.zeros((n, 3))
@@ -75,3 +78,21 @@ def test_long_window_blocks_match_the_whole_series(monkeypatch):
     assert math.isclose(f["dcd_rel_vs_f64"], (f["cd"] - r["cd"]) / r["cd"], rel_tol=1e-12)
     assert math.isclose(f["dcd_rel_vs_f64_sem"],
                         math.hypot(f["cd_sem"], r["cd_sem"]) / r["cd"], rel_tol=1e-12)
+
+
+def test_long_window_noise_seed_keeps_the_body(monkeypatch):
+    """--seed re-seeds the initial velocity noise of the workload's lattice
+    (its body built from the workload's own seed) and is recorded."""
+    made = []
+
+    def fake_setup(wl, storage, mm="fast", kernel="auto"):
+        assert wl["seed"] == bench.WORKLOADS["channel256"]["seed"]
+        made.append(FakeLattice(0.2))
+        return made[-1]
+
+    monkeypatch.setattr(bench, "setup_gpu", fake_setup)
+    wl = bench.WORKLOADS["channel256"]
+    out = bench.long_window_accuracy(wl, 4000, spinup=10, block=1000, forms=["f32"],
+                                     noise_seed=4321)
+    assert out["seed"] == 4321
+    assert made[0].noise == (4321, wl["amp"])
