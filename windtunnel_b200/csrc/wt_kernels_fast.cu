@@ -26,18 +26,20 @@ void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool, cudaStream_t s)
   k_step_lean<__half><<<grid, STEP_BX, 0, s>>>(a);
 }
 
+template <class S>
 inline dim3 pair_grid(int nx, int ny, int nz) {
-  return dim3((unsigned)((nx + 2 * PAIR_BX - 1) / (2 * PAIR_BX)), (unsigned)ny, (unsigned)nz);
+  constexpr int seg = 2 * pair_bx<S>();   // cells per block
+  return dim3((unsigned)((nx + seg - 1) / seg), (unsigned)ny, (unsigned)nz);
 }
 
 void launch_pair_f16(const StepArgs<__half>& a, dim3, bool, cudaStream_t s) {
-  const dim3 g = pair_grid(a.nx, a.ny, a.nz);
-  if (a.f16_sr) k_step_pair<__half, true><<<g, PAIR_BX, 0, s>>>(a);
-  else k_step_pair<__half, false><<<g, PAIR_BX, 0, s>>>(a);
+  const dim3 g = pair_grid<__half>(a.nx, a.ny, a.nz);
+  if (a.f16_sr) k_step_pair<__half, true><<<g, pair_bx<__half>(), 0, s>>>(a);
+  else k_step_pair<__half, false><<<g, pair_bx<__half>(), 0, s>>>(a);
 }
 
 void launch_pair_f32(const StepArgs<float>& a, dim3, bool, cudaStream_t s) {
-  k_step_pair<float, false><<<pair_grid(a.nx, a.ny, a.nz), PAIR_BX, 0, s>>>(a);
+  k_step_pair<float, false><<<pair_grid<float>(a.nx, a.ny, a.nz), pair_bx<float>(), 0, s>>>(a);
 }
 
 // ---- partial bounce-back and adjoint (float32 arithmetic) -------------------------

@@ -7,7 +7,7 @@
 // (_boundaries), the collision of collide_x2 (js/lbm.js:377-460
 // re-associated over opposite pairs) in the storage's scaled units.
 //
-// Thread t of block b owns cells x0 = 2 (b*PAIR_BX + t) and x0 + 1 of row
+// Thread t of block b owns cells x0 = 2 (b*pair_bx + t) and x0 + 1 of row
 // (y, z); nx is even, so every 32-bit word (x0, x0+1) of a population plane
 // is aligned. What the layout of the work buys, per pair of cells:
 //   * one aligned load of the pair per direction (the x-shifted directions:
@@ -45,13 +45,17 @@
 
 namespace wt {
 
-constexpr int PAIR_BX = 64;          // threads per block: 128 cells of one row
-// Resident blocks per SM the register budget is set for, the fastest measured
-// on B200: half storage 14 (72 registers, 28 warps; 55.2k MLUPS on the
-// 256x128x128 channel against 53.6k at 12 blocks and 80 registers), float32
-// storage 12 (80 registers, no spills; 40.3k against 40.0k at 14).
+// Threads per block (each block one x-segment of one row, two cells per
+// thread) and the resident blocks per SM the register budget is set for, the
+// fastest measured on B200: half storage 64 threads x 14 blocks (72
+// registers, 28 warps; 55.2k MLUPS on the 256x128x128 channel against 53.6k
+// at 12 blocks and 80 registers, 1-2% slower with 32 or 128 threads), float32
+// storage 128 threads x 6 blocks (80 registers, no spills, 24 warps; 40.7k
+// against 40.2k with 64 threads x 12 blocks).
 template <class S>
-constexpr int pair_min_blocks() { return sizeof(S) == 2 ? 14 : 12; }
+constexpr int pair_bx() { return sizeof(S) == 2 ? 64 : 128; }
+template <class S>
+constexpr int pair_min_blocks() { return sizeof(S) == 2 ? 14 : 6; }
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
   return __byte_perm(a, b, sel);
@@ -220,7 +224,7 @@ __device__ __forceinline__ void pair_force_partial(double fx, double fy, double 
   const int lane = threadIdx.x & 31;
   const unsigned half_bits = lane < 16 ? (any & 0xffffu) : (any >> 16);
   if ((lane & 15) == 0 && half_bits) {
-    const int x = 2 * (blockIdx.x * PAIR_BX + (threadIdx.x & ~15));
+    const int x = 2 * (blockIdx.x * pair_bx<S>() + (threadIdx.x & ~15));
     const int slot = a.wslot[seg_of(x, y, z, a.nx, a.ny)];
     if (slot >= 0) {
       a.part[3 * (size_t)slot] = fx;
@@ -486,12 +490,12 @@ put(qa + 1, psub(P, M));                            \
 }
 
 template <class S, bool SR>
-__global__ void __launch_bounds__(PAIR_BX, pair_min_blocks<S>())
+__global__ void __launch_bounds__(pair_bx<S>(), pair_min_blocks<S>())
     k_step_pair(const __grid_constant__ StepArgs<S> a) {
   using IO = PairIO<S>;
   using W = typename IO::W;
   constexpr float SC = IO::SC;
-  const int x0 = 2 * (blockIdx.x * PAIR_BX + threadIdx.x);
+  const int x0 = 2 * (blockIdx.x * pair_bx<S>() + threadIdx.x);
   const int y = blockIdx.y, z = blockIdx.z;
   const long long i0 = (long long)x0 + (long long)a.nx * y + a.nxy * z;
   const bool active = x0 < a.nx;
