@@ -2,6 +2,8 @@
 // parameter blocks shared by every kernel of libwt.so.
 #pragma once
 
+#include <utility>
+
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -151,6 +153,34 @@ __device__ __forceinline__ void prefetch_ahead(const StepArgs<S>& a, long long w
   if (a.pf <= 0 || lane >= 19) return;
   const long long e = warp_cell0 + a.pf + a.src[lane];
   if (e >= 0 && e < 19 * a.n) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.F + e));
+}
+
+// Programmatic dependent launch. A step kernel launched by launch_pdl (the
+// programmatic stream-serialization attribute) may have its blocks
+// dispatched into the SM slots the previous grid in the stream frees while
+// that grid's last blocks still run; pdl_enter, the kernel's first
+// statement, waits until the previous grid has completed and its stores are
+// visible, then lets the next grid launch. Launched without the attribute
+// both instructions return at once. A launch error is recorded for
+// cudaGetLastError like that of any launch.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <class... P, class... A>
+inline void launch_pdl(void (*k)(P...), dim3 grid, dim3 block, cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
 }
 
 // Block shape of the fused step: one thread per cell along x.

@@ -32,24 +32,14 @@ inline dim3 pair_grid(int nx, int ny, int nz) {
   return dim3((unsigned)((nx + seg - 1) / seg), (unsigned)ny, (unsigned)nz);
 }
 
-// The pair steps launch with programmatic stream serialization: a step's
-// blocks fill the slots the previous step's tail frees and start the moment
-// it completes (griddepcontrol in k_step_pair). Measured on B200: float32
-// +2.5% on 256x128x128, half storage +1-2%. A launch error is recorded for
-// cudaGetLastError like that of any launch.
+// The pair steps and the partial-bounce-back steps of the fast forms launch
+// with programmatic dependent launch (launch_pdl): a step's blocks fill the
+// slots the previous step's tail frees and start the moment it completes.
+// Measured on B200: pair float32 +2.5% on 256x128x128, half storage +1-2%;
+// the partial-bounce-back step on 128x64x64 +10%.
 template <class S>
 void launch_pair_pdl(void (*k)(StepArgs<S>), const StepArgs<S>& a, cudaStream_t s) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = pair_grid<S>(a.nx, a.ny, a.nz);
-  cfg.blockDim = dim3(pair_bx<S>());
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k, a);
+  launch_pdl(k, pair_grid<S>(a.nx, a.ny, a.nz), dim3(pair_bx<S>()), s, a);
 }
 
 void launch_pair_f16(const StepArgs<__half>& a, dim3, bool, cudaStream_t s) {
@@ -64,13 +54,13 @@ void launch_pair_f32(const StepArgs<float>& a, dim3, bool, cudaStream_t s) {
 // ---- partial bounce-back and adjoint (float32 arithmetic) -------------------------
 
 void launch_pbb_f32_fast(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s) {
-  if (wide) k_step_pbb<float, false, long long><<<grid, STEP_BX, 0, s>>>(a);
-  else k_step_pbb<float, false, int><<<grid, STEP_BX, 0, s>>>(a);
+  if (wide) launch_pdl(k_step_pbb<float, false, long long>, grid, dim3(STEP_BX), s, a);
+  else launch_pdl(k_step_pbb<float, false, int>, grid, dim3(STEP_BX), s, a);
 }
 
 void launch_pbb_f16_fast(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s) {
-  if (wide) k_step_pbb<__half, false, long long><<<grid, STEP_BX, 0, s>>>(a);
-  else k_step_pbb<__half, false, int><<<grid, STEP_BX, 0, s>>>(a);
+  if (wide) launch_pdl(k_step_pbb<__half, false, long long>, grid, dim3(STEP_BX), s, a);
+  else launch_pdl(k_step_pbb<__half, false, int>, grid, dim3(STEP_BX), s, a);
 }
 
 void launch_adj_f32(const StepArgs<float>& a, const float* Tn, float* Tc, double* ds, double wJ,

@@ -495,13 +495,7 @@ __global__ void __launch_bounds__(pair_bx<S>(), pair_min_blocks<S>())
   using IO = PairIO<S>;
   using W = typename IO::W;
   constexpr float SC = IO::SC;
-  // Programmatic dependent launch (the launch sets the stream-serialization
-  // attribute): this grid's blocks may be dispatched into the SM slots the
-  // previous grid's last blocks free; each waits here until that grid has
-  // completed and its stores are visible, then lets the next grid launch.
-  // Without the attribute both instructions return at once.
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  pdl_enter();   // programmatic dependent launch (launch_pdl)
   const int x0 = 2 * (blockIdx.x * pair_bx<S>() + threadIdx.x);
   const int y = blockIdx.y, z = blockIdx.z;
   const long long i0 = (long long)x0 + (long long)a.nx * y + a.nxy * z;

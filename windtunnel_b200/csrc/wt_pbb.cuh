@@ -350,6 +350,7 @@ __device__ __forceinline__ S to_store(T v) {
 template <class S, bool EXACT, class IDX>
 __global__ void __launch_bounds__(STEP_BX) k_step_pbb(const __grid_constant__ StepArgs<S> a) {
   using M = typename std::conditional<EXACT, double, float>::type;
+  pdl_enter();
   const int x = blockIdx.x * STEP_BX + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
   const long long i = (long long)x + (long long)a.nx * y + a.nxy * z;
@@ -496,6 +497,7 @@ constexpr int adj_min_blocks() { return sizeof(T) == 8 ? 3 : (sizeof(S) == 4 ? 4
 template <class S, class T, bool NB>
 __global__ void __launch_bounds__(STEP_BX, adj_min_blocks<S, T>()) k_adjoint(const __grid_constant__ StepArgs<S> a,
                                                          const __grid_constant__ AdjArgs<T> j) {
+  pdl_enter();
   const int x = blockIdx.x * STEP_BX + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
   const long long i = (long long)x + (long long)a.nx * y + a.nxy * z;
@@ -659,8 +661,8 @@ inline void launch_adjoint(const StepArgs<S>& a, const T* Tn, T* Tc, double* ds,
     j.rowb[q] = nb ? (uint32_t)(q * a.n * (long long)sizeof(T)) : 0u;
   }
   const dim3 grid = step_grid(a.nx, a.ny, a.nz);
-  if (nb) k_adjoint<S, T, true><<<grid, STEP_BX, 0, s>>>(a, j);
-  else k_adjoint<S, T, false><<<grid, STEP_BX, 0, s>>>(a, j);
+  if (nb) launch_pdl(k_adjoint<S, T, true>, grid, dim3(STEP_BX), s, a, j);
+  else launch_pdl(k_adjoint<S, T, false>, grid, dim3(STEP_BX), s, a, j);
 }
 
 }  // namespace wt
