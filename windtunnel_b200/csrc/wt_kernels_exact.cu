@@ -12,23 +12,23 @@
 namespace wt {
 
 void launch_step_f32_exact(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s) {
-  if (wide) k_step<float, true, long long><<<grid, STEP_BX, 0, s>>>(a);
-  else k_step<float, true, int><<<grid, STEP_BX, 0, s>>>(a);
+  if (wide) launch_pdl(k_step<float, true, long long>, grid, dim3(STEP_BX), s, a);
+  else launch_pdl(k_step<float, true, int>, grid, dim3(STEP_BX), s, a);
 }
 
 void launch_step_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cudaStream_t s) {
-  if (wide) k_step<double, true, long long><<<grid, STEP_BX, 0, s>>>(a);
-  else k_step<double, true, int><<<grid, STEP_BX, 0, s>>>(a);
+  if (wide) launch_pdl(k_step<double, true, long long>, grid, dim3(STEP_BX), s, a);
+  else launch_pdl(k_step<double, true, int>, grid, dim3(STEP_BX), s, a);
 }
 
 void launch_pbb_f32_exact(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s) {
-  if (wide) k_step_pbb<float, true, long long><<<grid, STEP_BX, 0, s>>>(a);
-  else k_step_pbb<float, true, int><<<grid, STEP_BX, 0, s>>>(a);
+  if (wide) launch_pdl(k_step_pbb<float, true, long long>, grid, dim3(STEP_BX), s, a);
+  else launch_pdl(k_step_pbb<float, true, int>, grid, dim3(STEP_BX), s, a);
 }
 
 void launch_pbb_f64_exact(const StepArgs<double>& a, dim3 grid, bool wide, cudaStream_t s) {
-  if (wide) k_step_pbb<double, true, long long><<<grid, STEP_BX, 0, s>>>(a);
-  else k_step_pbb<double, true, int><<<grid, STEP_BX, 0, s>>>(a);
+  if (wide) launch_pdl(k_step_pbb<double, true, long long>, grid, dim3(STEP_BX), s, a);
+  else launch_pdl(k_step_pbb<double, true, int>, grid, dim3(STEP_BX), s, a);
 }
 
 void launch_adj_f32x(const StepArgs<float>& a, const double* Tn, double* Tc, double* ds,

@@ -9,21 +9,21 @@
 namespace wt {
 
 void launch_step_f32_fast(const StepArgs<float>& a, dim3 grid, bool wide, cudaStream_t s) {
-  if (wide) k_step<float, false, long long><<<grid, STEP_BX, 0, s>>>(a);
-  else k_step<float, false, int><<<grid, STEP_BX, 0, s>>>(a);
+  if (wide) launch_pdl(k_step<float, false, long long>, grid, dim3(STEP_BX), s, a);
+  else launch_pdl(k_step<float, false, int>, grid, dim3(STEP_BX), s, a);
 }
 
 void launch_step_f16_fast(const StepArgs<__half>& a, dim3 grid, bool wide, cudaStream_t s) {
-  if (wide) k_step<__half, false, long long><<<grid, STEP_BX, 0, s>>>(a);
-  else k_step<__half, false, int><<<grid, STEP_BX, 0, s>>>(a);
+  if (wide) launch_pdl(k_step<__half, false, long long>, grid, dim3(STEP_BX), s, a);
+  else launch_pdl(k_step<__half, false, int>, grid, dim3(STEP_BX), s, a);
 }
 
 void launch_lean_f32(const StepArgs<float>& a, dim3 grid, bool, cudaStream_t s) {
-  k_step_lean<float><<<grid, STEP_BX, 0, s>>>(a);
+  launch_pdl(k_step_lean<float>, grid, dim3(STEP_BX), s, a);
 }
 
 void launch_lean_f16(const StepArgs<__half>& a, dim3 grid, bool, cudaStream_t s) {
-  k_step_lean<__half><<<grid, STEP_BX, 0, s>>>(a);
+  launch_pdl(k_step_lean<__half>, grid, dim3(STEP_BX), s, a);
 }
 
 template <class S>
@@ -32,11 +32,11 @@ inline dim3 pair_grid(int nx, int ny, int nz) {
   return dim3((unsigned)((nx + seg - 1) / seg), (unsigned)ny, (unsigned)nz);
 }
 
-// The pair steps and the partial-bounce-back steps of the fast forms launch
-// with programmatic dependent launch (launch_pdl): a step's blocks fill the
-// slots the previous step's tail frees and start the moment it completes.
-// Measured on B200: pair float32 +2.5% on 256x128x128, half storage +1-2%;
-// the partial-bounce-back step on 128x64x64 +10%.
+// Every step kernel (direct, lean, pair, partial bounce-back, adjoint)
+// launches with programmatic dependent launch (launch_pdl): a step's blocks
+// fill the slots the previous step's tail frees and start the moment it
+// completes. Measured on B200: pair float32 +2.5% on 256x128x128, half
+// storage +1-2%; the partial-bounce-back step on 128x64x64 +10%.
 template <class S>
 void launch_pair_pdl(void (*k)(StepArgs<S>), const StepArgs<S>& a, cudaStream_t s) {
   launch_pdl(k, pair_grid<S>(a.nx, a.ny, a.nz), dim3(pair_bx<S>()), s, a);

@@ -37,6 +37,7 @@ constexpr int lean_min_blocks() { return sizeof(S) == 4 ? 7 : 8; }
 template <class S>
 __global__ void __launch_bounds__(STEP_BX, lean_min_blocks<S>())
     k_step_lean(const __grid_constant__ StepArgs<S> a) {
+  pdl_enter();   // programmatic dependent launch (launch_pdl)
   using T = X2<S>;
   constexpr float SC = T::SC;
   const int x = blockIdx.x * STEP_BX + threadIdx.x;

@@ -355,6 +355,7 @@ constexpr int step_min_blocks(bool exact) { return exact ? 4 : 8; }
 template <class S, bool EXACT, class IDX>
 __global__ void __launch_bounds__(STEP_BX, step_min_blocks(EXACT)) k_step(const __grid_constant__ StepArgs<S> a) {
   using M = typename std::conditional<EXACT, double, float>::type;
+  pdl_enter();   // programmatic dependent launch (launch_pdl)
   const int x = blockIdx.x * STEP_BX + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
   const long long i = (long long)x + (long long)a.nx * y + a.nxy * z;
