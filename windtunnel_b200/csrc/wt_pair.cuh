@@ -47,15 +47,15 @@ namespace wt {
 
 // Threads per block (each block one x-segment of one row, two cells per
 // thread) and the resident blocks per SM the register budget is set for, the
-// fastest measured on B200: half storage 64 threads x 14 blocks (72
-// registers, 28 warps; 55.2k MLUPS on the 256x128x128 channel against 53.6k
-// at 12 blocks and 80 registers, 1-2% slower with 32 or 128 threads), float32
-// storage 128 threads x 6 blocks (80 registers, no spills, 24 warps; 40.7k
-// against 40.2k with 64 threads x 12 blocks).
+// fastest measured on B200 (launched with programmatic dependent launch):
+// 128 threads for both storages; half storage 7 blocks (72 registers, 28
+// warps; 80 registers at 24 warps lose 3%; 64-thread blocks 0.9% and 32-thread
+// blocks 8% slower), float32 storage 6 blocks (80 registers, no spills, 24
+// warps; 64-thread blocks 1.5% slower).
 template <class S>
-constexpr int pair_bx() { return sizeof(S) == 2 ? 64 : 128; }
+constexpr int pair_bx() { return 128; }
 template <class S>
-constexpr int pair_min_blocks() { return sizeof(S) == 2 ? 14 : 6; }
+constexpr int pair_min_blocks() { return sizeof(S) == 2 ? 7 : 6; }
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
   return __byte_perm(a, b, sel);
